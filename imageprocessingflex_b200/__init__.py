@@ -1,0 +1,26 @@
+"""B200-native (sm_100a) neighbourhood-filter path of ImageProcessingFlex.
+
+``from imageprocessingflex_b200 import gaussianBlur, BorderMode`` mirrors the
+reference's ``ipf::gaussianBlur`` etc. on numpy arrays (host) and CUDA torch
+tensors (device).  The C++ form is ``include/ipf_cuda.hpp``; the C ABI is
+``include/ipfc.h``; the kernels live in ``csrc/``.
+"""
+from .filters import (  # noqa: F401
+    BorderMode,
+    Error,
+    MorphShape,
+    blur,
+    boxFilter,
+    derivKernel,
+    dilate,
+    erode,
+    filter2D,
+    gaussianBlur,
+    gaussianKernel1D,
+    getStructuringElement,
+    medianBlur,
+    sepFilter2D,
+    sobel,
+)
+
+__version__ = "1.0.0"

@@ -1,0 +1,83 @@
+"""ctypes binding of ``libipfcuda.so`` (the C ABI declared in include/ipfc.h).
+
+The library is built in-tree by ``imageprocessingflex_b200.build``.  Loading
+fails loudly (``ImportError``) when it is missing and cannot be built: there is
+no CPU fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import build as _build
+
+c_int, c_double, c_void_p, c_longlong = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
+
+
+class IpfcImage(ctypes.Structure):
+    """Mirror of ``struct ipfc_image``."""
+
+    _fields_ = [
+        ("data", c_void_p),
+        ("width", c_int),
+        ("height", c_int),
+        ("channels", c_int),
+        ("dtype", c_int),
+        ("pitch", c_longlong),
+        ("mem", c_int),
+    ]
+
+
+IMG_P = ctypes.POINTER(IpfcImage)
+DBL_P = ctypes.POINTER(c_double)
+
+# name -> (restype, argtypes)
+_SIGNATURES = {
+    "ipfc_last_error": (ctypes.c_char_p, []),
+    "ipfc_version": (c_int, []),
+    "ipfc_gaussian_kernel_1d": (c_int, [c_double, c_int, c_void_p, c_int]),
+    "ipfc_deriv_kernel": (c_int, [c_int, c_int, c_void_p, c_int]),
+    "ipfc_structuring_element": (c_int, [c_int, c_int, c_int, c_void_p]),
+    "ipfc_sep_filter2d": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int, c_double,
+                                  c_double, c_void_p]),
+    "ipfc_gaussian_blur": (c_int, [IMG_P, IMG_P, c_double, c_double, c_int, c_int, c_void_p]),
+    "ipfc_box_filter": (c_int, [IMG_P, IMG_P, c_int, c_int, c_int, c_int, c_double, c_void_p]),
+    "ipfc_sobel": (c_int, [IMG_P, IMG_P, c_int, c_int, c_int, c_double, c_int, c_void_p]),
+    "ipfc_filter2d": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_double,
+                              c_void_p]),
+    "ipfc_median_blur": (c_int, [IMG_P, IMG_P, c_int, c_int, c_void_p]),
+    "ipfc_erode": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "ipfc_dilate": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "ipfc_probe_border_index": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "ipfc_probe_saturate": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p]),
+}
+
+_lib = None
+
+
+def library_path() -> str:
+    return _build.LIBPATH
+
+
+def load() -> ctypes.CDLL:
+    """Loads (building first if needed) and returns the CUDA library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIBPATH
+    if not os.path.exists(path) or os.environ.get("IPFC_REBUILD") == "1":
+        try:
+            _build.build()
+        except Exception as exc:  # toolchain missing or compile error
+            raise ImportError(f"libipfcuda.so is missing and could not be built: {exc}") from exc
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_names():
+    return list(_SIGNATURES)

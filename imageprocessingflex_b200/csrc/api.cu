@@ -1,0 +1,592 @@
+// api.cu -- the extern "C" entry points of include/ipfc.h.
+//
+// Host responsibilities: argument checks with the reference's messages, tap
+// generation in FP64 exactly as the reference computes it, staging of host
+// images through stream-ordered device allocations, and dispatch to the
+// kernels.  No compute runs on the host and nothing falls back to it.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ipfc.h"
+#include "kernels.cuh"
+
+namespace ipfc {
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_status(cudaError_t e, const char* fn) {
+    if (e == cudaSuccess) return IPFC_OK;
+    cudaGetLastError();  // clear sticky-free errors so the next call starts clean
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(IPFC_ERR_NOMEM, "ipf: %s: device allocation failed (%s)", fn, cudaGetErrorString(e));
+    return set_error(IPFC_ERR_CUDA, "ipf: %s: CUDA error: %s", fn, cudaGetErrorString(e));
+}
+
+#define IPFC_TRY_CUDA(expr, fn)                          \
+    do {                                                  \
+        cudaError_t e_ = (expr);                          \
+        if (e_ != cudaSuccess) return cuda_status(e_, fn); \
+    } while (0)
+
+size_t elem_bytes(int dt) {
+    switch (dt) {
+        case IPFC_U8: return 1;
+        case IPFC_U16: case IPFC_I16: return 2;
+        case IPFC_I32: case IPFC_F32: return 4;
+        case IPFC_F64: return 8;
+        default: return 0;
+    }
+}
+
+static bool dtype_supported(int dt) { return dt == IPFC_U8 || dt == IPFC_U16 || dt == IPFC_I16 || dt == IPFC_F32; }
+
+static long long row_bytes(const ipfc_image* im) {
+    return (long long)im->width * im->channels * (long long)elem_bytes(im->dtype);
+}
+
+static long long pitch_of(const ipfc_image* im) { return im->pitch > 0 ? im->pitch : row_bytes(im); }
+
+// ---------------------------------------------------------------------------
+// Device memory: stream-ordered allocations from the device's default pool,
+// kept cached by a maximal release threshold (set once per device) so that
+// steady-state calls do not return memory to the driver.
+// ---------------------------------------------------------------------------
+static unsigned g_pool_ready = 0;
+
+cudaError_t prepare_device() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned bit = 1u << (dev & 31);
+    if (__atomic_load_n(&g_pool_ready, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
+    cudaMemPool_t pool;
+    e = cudaDeviceGetDefaultMemPool(&pool, dev);
+    if (e != cudaSuccess) return e;
+    unsigned long long thr = ~0ull;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    if (e != cudaSuccess) return e;
+    __atomic_fetch_or(&g_pool_ready, bit, __ATOMIC_ACQ_REL);
+    return cudaSuccess;
+}
+
+// A device view of an image: the caller's memory, or a staged copy.
+struct DevView {
+    void* ptr = nullptr;
+    long long pitch = 0;
+    bool owned = false;
+};
+
+static long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+static int view_in(const ipfc_image* im, cudaStream_t s, DevView* v, const char* fn) {
+    if (im->mem == IPFC_MEM_DEVICE) {
+        v->ptr = im->data;
+        v->pitch = pitch_of(im);
+        return IPFC_OK;
+    }
+    const long long rb = row_bytes(im);
+    v->pitch = round_up(rb > 0 ? rb : 1, 128);
+    IPFC_TRY_CUDA(cudaMallocAsync(&v->ptr, (size_t)(v->pitch * im->height), s), fn);
+    v->owned = true;
+    IPFC_TRY_CUDA(cudaMemcpy2DAsync(v->ptr, (size_t)v->pitch, im->data, (size_t)pitch_of(im), (size_t)rb,
+                                    (size_t)im->height, cudaMemcpyHostToDevice, s),
+                  fn);
+    return IPFC_OK;
+}
+
+static int view_out(const ipfc_image* im, cudaStream_t s, DevView* v, const char* fn) {
+    if (im->mem == IPFC_MEM_DEVICE) {
+        v->ptr = im->data;
+        v->pitch = pitch_of(im);
+        return IPFC_OK;
+    }
+    const long long rb = row_bytes(im);
+    v->pitch = round_up(rb > 0 ? rb : 1, 128);
+    IPFC_TRY_CUDA(cudaMallocAsync(&v->ptr, (size_t)(v->pitch * im->height), s), fn);
+    v->owned = true;
+    return IPFC_OK;
+}
+
+// Copies a staged result back to host memory, releases staging memory and,
+// when any side lives in host memory, waits for the stream.
+static int finish(const ipfc_image* dst, DevView* in, DevView* out, cudaStream_t s, const char* fn) {
+    cudaError_t e = cudaSuccess;
+    if (out->owned) {
+        e = cudaMemcpy2DAsync(dst->data, (size_t)pitch_of(dst), out->ptr, (size_t)out->pitch, (size_t)row_bytes(dst),
+                              (size_t)dst->height, cudaMemcpyDeviceToHost, s);
+    }
+    if (in && in->owned) cudaFreeAsync(in->ptr, s);
+    if (out->owned) cudaFreeAsync(out->ptr, s);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    if ((in && in->owned) || out->owned) IPFC_TRY_CUDA(cudaStreamSynchronize(s), fn);
+    return IPFC_OK;
+}
+
+// Common checks: both views non-null, supported types, equal shapes, no
+// aliasing, a device present.  Returns IPFC_OK, an error, or -1 for "empty
+// image: nothing to do" (the reference returns an empty result).
+static int check_pair(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type) {
+    if (!src || !dst) return set_error(IPFC_ERR_INVALID, "ipf: %s: null image", fn);
+    if (src->width < 0 || src->height < 0 || src->channels < 1)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid source dimensions", fn);
+    if (dst->width != src->width || dst->height != src->height || dst->channels != src->channels)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: destination shape does not match source", fn);
+    if (!dtype_supported(src->dtype) || !dtype_supported(dst->dtype))
+        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: element type not provided by this build (u8, u16, i16, f32)",
+                         fn);
+    if (same_type && src->dtype != dst->dtype)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: source and destination types differ", fn);
+    if ((src->mem != IPFC_MEM_HOST && src->mem != IPFC_MEM_DEVICE) ||
+        (dst->mem != IPFC_MEM_HOST && dst->mem != IPFC_MEM_DEVICE))
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid memory kind", fn);
+    if ((src->pitch != 0 && src->pitch < row_bytes(src)) || (dst->pitch != 0 && dst->pitch < row_bytes(dst)))
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: pitch smaller than a row", fn);
+    if ((long long)src->width * src->channels > 0x3fffffffLL || (long long)src->height > 0x3fffffffLL)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: image too large", fn);
+    if (src->width == 0 || src->height == 0) return -1;
+    if (!src->data || !dst->data) return set_error(IPFC_ERR_INVALID, "ipf: %s: null pixel pointer", fn);
+    if (src->data == dst->data) return set_error(IPFC_ERR_INVALID, "ipf: %s: in-place operation is not supported", fn);
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return set_error(IPFC_ERR_CUDA, "ipf: %s: no CUDA device available", fn);
+    }
+    cudaError_t e = prepare_device();
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    return IPFC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tap generators (FP64, the reference's expressions and order)
+// ---------------------------------------------------------------------------
+int gaussian_taps(double sigma, int ksize, std::vector<double>& k) {
+    if (ksize <= 0) {
+        if (!(sigma > 0))
+            return set_error(IPFC_ERR_INVALID, "ipf: gaussianKernel1D: need sigma > 0 or ksize > 0");
+        const int r = static_cast<int>(3.0 * sigma + 0.5);
+        ksize = 2 * (r > 1 ? r : 1) + 1;
+    }
+    if (ksize % 2 != 1) return set_error(IPFC_ERR_INVALID, "ipf: gaussianKernel1D: ksize must be odd");
+    if (sigma <= 0) sigma = 0.3 * ((ksize - 1) * 0.5 - 1) + 0.8;
+    k.assign((size_t)ksize, 0.0);
+    const int c = ksize / 2;
+    double sum = 0;
+    for (int i = 0; i < ksize; ++i) {
+        k[i] = std::exp(-0.5 * (i - c) * (i - c) / (sigma * sigma));
+        sum += k[i];
+    }
+    for (double& v : k) v /= sum;
+    return IPFC_OK;
+}
+
+int deriv_taps(int order, int ksize, std::vector<double>& k) {
+    if (ksize == 1) {
+        if (order == 0) { k = {1.0}; return IPFC_OK; }
+        if (order == 1) { k = {-1.0, 0.0, 1.0}; return IPFC_OK; }
+        if (order == 2) { k = {1.0, -2.0, 1.0}; return IPFC_OK; }
+        return set_error(IPFC_ERR_INVALID, "ipf: derivKernel: order > 2 requires ksize >= 3");
+    }
+    if (!(ksize % 2 == 1 && ksize >= 3 && ksize <= 31))
+        return set_error(IPFC_ERR_INVALID, "ipf: derivKernel: ksize must be odd in [3, 31]");
+    if (!(order >= 0 && order < ksize)) return set_error(IPFC_ERR_INVALID, "ipf: derivKernel: invalid derivative order");
+    // binomial smoothing (1, 1)^(ksize-1-order) convolved with (-1, 1)^order
+    k.assign(1, 1.0);
+    for (int step = 0; step < ksize - 1; ++step) {
+        const double a = step < ksize - 1 - order ? 1.0 : -1.0;
+        std::vector<double> r(k.size() + 1, 0.0);
+        for (size_t i = 0; i < k.size(); ++i) {
+            r[i] += k[i] * a;
+            r[i + 1] += k[i] * 1.0;
+        }
+        k.swap(r);
+    }
+    return IPFC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Separable path shared by sepFilter2D, gaussianBlur and sobel.
+// ---------------------------------------------------------------------------
+static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh, int ax,
+                   int ay, int border, double delta, double bv, cudaStream_t s, const char* fn) {
+    if (!kx || !ky || kw <= 0 || kh <= 0)
+        return set_error(IPFC_ERR_INVALID, "ipf: separable filter: empty kernel");
+    if (border < IPFC_BORDER_CONSTANT || border > IPFC_BORDER_WRAP)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid border mode", fn);
+    if (ax < 0) ax = kw / 2;
+    if (ay < 0) ay = kh / 2;
+    if (ax >= kw || ay >= kh) return set_error(IPFC_ERR_INVALID, "ipf: %s: anchor outside kernel", fn);
+    int rc = check_pair(src, dst, fn, false);
+    if (rc == -1) return IPFC_OK;
+    if (rc) return rc;
+    SepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.W = src->width;
+    a.H = src->height;
+    a.C = src->channels;
+    a.kw = kw;
+    a.kh = kh;
+    a.ax = ax;
+    a.ay = ay;
+    a.border = border;
+    a.delta = (float)delta;
+    a.bv = (float)bv;
+    for (int i = 0; i < kw && i < kSepMaxParamTaps; ++i) a.kx[i] = (float)kx[i];
+    for (int j = 0; j < kh && j < kSepMaxParamTaps; ++j) a.ky[j] = (float)ky[j];
+    DevView in, out;
+    if ((rc = view_in(src, s, &in, fn))) return rc;
+    if ((rc = view_out(dst, s, &out, fn))) {
+        finish(dst, &in, &out, s, fn);
+        return rc;
+    }
+    a.src = in.ptr;
+    a.spitch = in.pitch;
+    a.dst = out.ptr;
+    a.dpitch = out.pitch;
+    float* dtaps = nullptr;
+    float* scratch = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (sep_needs_scratch(a)) {
+        std::vector<float> taps((size_t)kw + kh);
+        for (int i = 0; i < kw; ++i) taps[i] = (float)kx[i];
+        for (int j = 0; j < kh; ++j) taps[kw + j] = (float)ky[j];
+        e = cudaMallocAsync((void**)&dtaps, taps.size() * sizeof(float), s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dtaps, taps.data(), taps.size() * sizeof(float),
+                                                  cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMallocAsync((void**)&scratch, sizeof(float) * (size_t)a.W * a.C * a.H, s);
+    }
+    if (e == cudaSuccess) e = sep_launch(src->dtype, dst->dtype, a, dtaps, dtaps ? dtaps + kw : nullptr, scratch, s);
+    if (dtaps) cudaFreeAsync(dtaps, s);
+    if (scratch) cudaFreeAsync(scratch, s);
+    rc = finish(dst, &in, &out, s, fn);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    return rc;
+}
+
+}  // namespace ipfc
+
+using namespace ipfc;
+
+extern "C" {
+
+const char* ipfc_last_error(void) { return g_last_error.c_str(); }
+
+int ipfc_version(void) { return (1 << 16) | (0 << 8) | 0; }
+
+int ipfc_gaussian_kernel_1d(double sigma, int ksize, double* out, int cap) {
+    std::vector<double> k;
+    if (gaussian_taps(sigma, ksize, k)) return -1;
+    for (int i = 0; i < (int)k.size() && i < cap; ++i) out[i] = k[i];
+    return (int)k.size();
+}
+
+int ipfc_deriv_kernel(int order, int ksize, double* out, int cap) {
+    std::vector<double> k;
+    if (deriv_taps(order, ksize, k)) return -1;
+    for (int i = 0; i < (int)k.size() && i < cap; ++i) out[i] = k[i];
+    return (int)k.size();
+}
+
+int ipfc_structuring_element(int shape, int width, int height, uint8_t* out) {
+    if (height <= 0) height = width;
+    if (width <= 0 || height <= 0)
+        return set_error(IPFC_ERR_INVALID, "ipf: getStructuringElement: size must be positive");
+    if (shape < IPFC_MORPH_RECT || shape > IPFC_MORPH_ELLIPSE)
+        return set_error(IPFC_ERR_INVALID, "ipf: getStructuringElement: invalid shape");
+    std::memset(out, 0, (size_t)width * height);
+    const int r = height / 2, c = width / 2;
+    const double inv_r2 = r ? 1.0 / (static_cast<double>(r) * r) : 0.0;
+    for (int i = 0; i < height; ++i) {
+        int j1 = 0, j2 = 0;
+        if (shape == IPFC_MORPH_RECT || (shape == IPFC_MORPH_CROSS && i == r)) {
+            j2 = width;
+        } else if (shape == IPFC_MORPH_CROSS) {
+            j1 = c;
+            j2 = c + 1;
+        } else {
+            const int dy = i - r;
+            if (std::abs(dy) <= r) {
+                const double v = c * std::sqrt((r * r - dy * dy) * inv_r2);
+                const int dx = (int)(v + 0.5);  // saturate_cast<int>: half away from zero, v >= 0
+                j1 = c - dx > 0 ? c - dx : 0;
+                j2 = c + dx + 1 < width ? c + dx + 1 : width;
+            }
+        }
+        for (int j = j1; j < j2; ++j) out[(size_t)i * width + j] = 1;
+    }
+    return IPFC_OK;
+}
+
+int ipfc_sep_filter2d(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh,
+                      int ax, int ay, int border, double delta, double border_value, void* stream) {
+    return run_sep(src, dst, kx, kw, ky, kh, ax, ay, border, delta, border_value, (cudaStream_t)stream,
+                   "sepFilter2D");
+}
+
+int ipfc_gaussian_blur(const ipfc_image* src, ipfc_image* dst, double sigma_x, double sigma_y, int ksize, int border,
+                       void* stream) {
+    if (sigma_y <= 0) sigma_y = sigma_x;
+    std::vector<double> kx, ky;
+    if (gaussian_taps(sigma_x, ksize, kx)) return IPFC_ERR_INVALID;
+    if (gaussian_taps(sigma_y, ksize, ky)) return IPFC_ERR_INVALID;
+    return run_sep(src, dst, kx.data(), (int)kx.size(), ky.data(), (int)ky.size(), -1, -1, border, 0.0, 0.0,
+                   (cudaStream_t)stream, "gaussianBlur");
+}
+
+int ipfc_sobel(const ipfc_image* src, ipfc_image* dst, int dx, int dy, int ksize, double scale, int border,
+               void* stream) {
+    if (!(dx >= 0 && dy >= 0 && dx + dy > 0)) return set_error(IPFC_ERR_INVALID, "ipf: sobel: need dx + dy > 0");
+    std::vector<double> kx, ky;
+    if (deriv_taps(dx, ksize, kx)) return IPFC_ERR_INVALID;
+    if (deriv_taps(dy, ksize, ky)) return IPFC_ERR_INVALID;
+    if (ksize == 1) {  // keep both kernels 3 long so the anchors stay centred (filter.hpp:401-404)
+        if (kx.size() == 1) kx = {0.0, 1.0, 0.0};
+        if (ky.size() == 1) ky = {0.0, 1.0, 0.0};
+    }
+    for (double& v : kx) v *= scale;
+    return run_sep(src, dst, kx.data(), (int)kx.size(), ky.data(), (int)ky.size(), -1, -1, border, 0.0, 0.0,
+                   (cudaStream_t)stream, "sobel");
+}
+
+int ipfc_box_filter(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int normalize, int border,
+                    double border_value, void* stream) {
+    const char* fn = "boxFilter";
+    if (kw <= 0 || kh <= 0) return set_error(IPFC_ERR_INVALID, "ipf: boxFilter: kernel size must be positive");
+    if (border < IPFC_BORDER_CONSTANT || border > IPFC_BORDER_WRAP)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid border mode", fn);
+    int rc = check_pair(src, dst, fn, false);
+    if (rc == -1) return IPFC_OK;
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.W = src->width;
+    a.H = src->height;
+    a.C = src->channels;
+    a.kw = kw;
+    a.kh = kh;
+    a.ax = kw / 2;
+    a.ay = kh / 2;
+    a.border = border;
+    a.normalize = normalize ? 1 : 0;
+    a.bv = (float)border_value;
+    const double n = (double)kw * kh;
+    const double scale = normalize ? 1.0 / n : 1.0;
+    a.scale_hi = (float)scale;
+    a.scale_lo = (float)(scale - (double)a.scale_hi);
+    const bool int_src = src->dtype != IPFC_F32;
+    const double maxval = src->dtype == IPFC_U8 ? 255.0 : (src->dtype == IPFC_U16 ? 65535.0 : 32768.0);
+    const bool bv_int = std::floor(border_value) == border_value && std::fabs(border_value) <= 65535.0;
+    const bool exact = int_src && bv_int && n * std::fmax(maxval, std::fabs(border_value)) < 2147483647.0;
+    if (exact && normalize && ((long long)kw * kh) % 2 == 0) {
+        // Outcome of each exact tie S/n = t + 1/2 under the reference's
+        // expression saturate_cast(S * (1.0 / n)) (filter.hpp:238, 246).
+        const long long nn = (long long)kw * kh;
+        const long long tmax = (long long)std::fmin(65535.0, std::fmax(maxval, std::fabs(border_value)));
+        for (long long t = 0; t <= tmax; ++t) {
+            const double S = (double)(nn * (2 * t + 1) / 2);
+            const double d = S * scale + 0.5;
+            if ((long long)d == t + 1) a.tie_up[t >> 5] |= 1u << (t & 31);
+        }
+    }
+    DevView in, out;
+    if ((rc = view_in(src, s, &in, fn))) return rc;
+    if ((rc = view_out(dst, s, &out, fn))) {
+        finish(dst, &in, &out, s, fn);
+        return rc;
+    }
+    a.src = in.ptr;
+    a.spitch = in.pitch;
+    a.dst = out.ptr;
+    a.dpitch = out.pitch;
+    cudaError_t e = box_launch(src->dtype, dst->dtype, a, exact, s);
+    rc = finish(dst, &in, &out, s, fn);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    return rc;
+}
+
+int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
+                  int border, double delta, double border_value, void* stream) {
+    const char* fn = "filter2D";
+    if (!kernel || kw <= 0 || kh <= 0)
+        return set_error(IPFC_ERR_INVALID, "ipf: filter2D: kernel must be a non-empty single-channel image");
+    if (ax < 0) ax = kw / 2;
+    if (ay < 0) ay = kh / 2;
+    if (!(ax < kw && ay < kh)) return set_error(IPFC_ERR_INVALID, "ipf: filter2D: anchor outside kernel");
+    if (border < IPFC_BORDER_CONSTANT || border > IPFC_BORDER_WRAP)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid border mode", fn);
+    int rc = check_pair(src, dst, fn, false);
+    if (rc == -1) return IPFC_OK;
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<float4> taps;
+    for (int j = 0; j < kh; ++j)
+        for (int i = 0; i < kw; ++i) {
+            const float w = kernel[(size_t)j * kw + i];
+            if (w != 0.f) taps.push_back(make_float4(w, (float)i, (float)j, 0.f));
+        }
+    F2DArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.W = src->width;
+    a.H = src->height;
+    a.C = src->channels;
+    a.kw = kw;
+    a.kh = kh;
+    a.ax = ax;
+    a.ay = ay;
+    a.border = border;
+    a.delta = (float)delta;
+    a.bv = (float)border_value;
+    a.ntaps = (int)taps.size();
+    a.dense = a.ntaps == kw * kh;
+    DevView in, out;
+    if ((rc = view_in(src, s, &in, fn))) return rc;
+    if ((rc = view_out(dst, s, &out, fn))) {
+        finish(dst, &in, &out, s, fn);
+        return rc;
+    }
+    a.src = in.ptr;
+    a.spitch = in.pitch;
+    a.dst = out.ptr;
+    a.dpitch = out.pitch;
+    float4* dtaps = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&dtaps, sizeof(float4) * (taps.size() ? taps.size() : 1), s);
+    if (e == cudaSuccess && !taps.empty())
+        e = cudaMemcpyAsync(dtaps, taps.data(), sizeof(float4) * taps.size(), cudaMemcpyHostToDevice, s);
+    a.taps = dtaps;
+    if (e == cudaSuccess) e = filter2d_launch(src->dtype, dst->dtype, a, s);
+    if (dtaps) cudaFreeAsync(dtaps, s);
+    rc = finish(dst, &in, &out, s, fn);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    return rc;
+}
+
+int ipfc_median_blur(const ipfc_image* src, ipfc_image* dst, int ksize, int border, void* stream) {
+    const char* fn = "medianBlur";
+    if (!(ksize >= 1 && ksize % 2 == 1))
+        return set_error(IPFC_ERR_INVALID, "ipf: medianBlur: ksize must be odd and positive");
+    if (border == IPFC_BORDER_CONSTANT)
+        return set_error(IPFC_ERR_INVALID, "ipf: medianBlur: Constant border is not supported");
+    if (border < IPFC_BORDER_CONSTANT || border > IPFC_BORDER_WRAP)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid border mode", fn);
+    int rc = check_pair(src, dst, fn, true);
+    if (rc == -1) return IPFC_OK;
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevView in, out;
+    if ((rc = view_in(src, s, &in, fn))) return rc;
+    if ((rc = view_out(dst, s, &out, fn))) {
+        finish(dst, &in, &out, s, fn);
+        return rc;
+    }
+    cudaError_t e;
+    if (ksize == 1) {  // the reference returns the source unchanged
+        e = cudaMemcpy2DAsync(out.ptr, (size_t)out.pitch, in.ptr, (size_t)in.pitch, (size_t)row_bytes(src),
+                              (size_t)src->height, cudaMemcpyDeviceToDevice, s);
+    } else {
+        MedianArgs a{in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, ksize, border};
+        e = median_launch(src->dtype, a, s);
+    }
+    rc = finish(dst, &in, &out, s, fn);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    return rc;
+}
+
+static int run_morph(const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int sw, int sh, int iterations,
+                     bool is_min, cudaStream_t s) {
+    const char* fn = is_min ? "erode" : "dilate";
+    if (!se || sw <= 0 || sh <= 0)
+        return set_error(IPFC_ERR_INVALID,
+                         "ipf: morphology: structuring element must be a non-empty single-channel mask");
+    int rc = check_pair(src, dst, fn, true);
+    if (rc == -1) return IPFC_OK;
+    if (rc) return rc;
+    MorphArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.W = src->width;
+    a.H = src->height;
+    a.C = src->channels;
+    a.sw = sw;
+    a.sh = sh;
+    a.ax = sw / 2;
+    a.ay = sh / 2;
+    a.is_min = is_min ? 1 : 0;
+    a.is_rect = 1;
+    for (int j = 0; j < sh; ++j)
+        for (int i = 0; i < sw; ++i) {
+            if (!se[(size_t)j * sw + i]) {
+                a.is_rect = 0;
+                continue;
+            }
+            if (a.noffs < kMorphMaxOffsets) a.offs[a.noffs] = make_short2((short)(i - a.ax), (short)(j - a.ay));
+            ++a.noffs;
+        }
+    if (!a.is_rect && a.noffs > kMorphMaxOffsets)
+        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: structuring element has more than %d members", fn,
+                         kMorphMaxOffsets);
+    DevView in, out;
+    if ((rc = view_in(src, s, &in, fn))) return rc;
+    if ((rc = view_out(dst, s, &out, fn))) {
+        finish(dst, &in, &out, s, fn);
+        return rc;
+    }
+    cudaError_t e = cudaSuccess;
+    const size_t rb = (size_t)row_bytes(src);
+    if (iterations <= 0) {
+        e = cudaMemcpy2DAsync(out.ptr, (size_t)out.pitch, in.ptr, (size_t)in.pitch, rb, (size_t)src->height,
+                              cudaMemcpyDeviceToDevice, s);
+    } else {
+        // Ping-pong: iteration i writes dst when (iterations - i) is even, so
+        // the last one lands in dst; the other buffer is scratch.
+        void* scratch = nullptr;
+        const long long sp = round_up((long long)rb, 128);
+        if (iterations > 1) e = cudaMallocAsync(&scratch, (size_t)(sp * src->height), s);
+        const void* cur = in.ptr;
+        long long cur_pitch = in.pitch;
+        for (int it = 1; it <= iterations && e == cudaSuccess; ++it) {
+            const bool to_dst = ((iterations - it) % 2) == 0;
+            a.src = cur;
+            a.spitch = cur_pitch;
+            a.dst = to_dst ? out.ptr : scratch;
+            a.dpitch = to_dst ? out.pitch : sp;
+            e = morph_launch(src->dtype, a, s);
+            cur = a.dst;
+            cur_pitch = a.dpitch;
+        }
+        if (scratch) cudaFreeAsync(scratch, s);
+    }
+    rc = finish(dst, &in, &out, s, fn);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    return rc;
+}
+
+int ipfc_erode(const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w, int se_h, int iterations,
+               void* stream) {
+    return run_morph(src, dst, se, se_w, se_h, iterations, true, (cudaStream_t)stream);
+}
+
+int ipfc_dilate(const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w, int se_h, int iterations,
+                void* stream) {
+    return run_morph(src, dst, se, se_w, se_h, iterations, false, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,298 @@
+"""Python mirror of ipf's neighbourhood-filter functions over the CUDA C ABI.
+
+Names, argument order, defaults and error texts follow the reference's free
+functions (include/ipf/filter.hpp, include/ipf/morphology.hpp).  The output
+type template parameter ``TOut`` of the reference is the ``dtype`` keyword.
+
+Images are ``numpy`` arrays shaped (H, W) or (H, W, C) -- host memory, the
+call copies in and out and returns a new array -- or CUDA ``torch`` tensors of
+the same shapes -- device memory, the call is asynchronous on ``stream``
+(default: torch's current stream) and returns a new tensor.  Every call runs
+on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+from enum import IntEnum
+
+import numpy as np
+
+from . import _lib
+
+
+class BorderMode(IntEnum):
+    """ipf::BorderMode (core.hpp:183)."""
+
+    Constant = 0
+    Replicate = 1
+    Reflect = 2
+    Reflect101 = 3
+    Wrap = 4
+
+
+class MorphShape(IntEnum):
+    """ipf::MorphShape (morphology.hpp:21)."""
+
+    Rect = 0
+    Cross = 1
+    Ellipse = 2
+
+
+class Error(RuntimeError):
+    """ipf::Error (core.hpp:35-38): every failure is reported with this type."""
+
+    def __init__(self, message: str, status: int = 1):
+        super().__init__(message)
+        self.status = status
+
+
+U8, U16, I16, I32, F32, F64 = range(6)
+_NP_CODE = {np.dtype(np.uint8): U8, np.dtype(np.uint16): U16, np.dtype(np.int16): I16,
+            np.dtype(np.int32): I32, np.dtype(np.float32): F32, np.dtype(np.float64): F64}
+_CODE_NP = {v: k for k, v in _NP_CODE.items()}
+MEM_HOST, MEM_DEVICE = 0, 1
+
+
+def _torch():
+    import torch  # imported lazily: host-array use needs no torch
+
+    return torch
+
+
+def _is_tensor(x) -> bool:
+    return type(x).__module__.startswith("torch") and hasattr(x, "is_cuda")
+
+
+def _torch_code(t) -> int:
+    torch = _torch()
+    table = {torch.uint8: U8, torch.uint16: U16, torch.int16: I16, torch.int32: I32,
+             torch.float32: F32, torch.float64: F64}
+    if t.dtype not in table:
+        raise Error(f"ipf: unsupported tensor dtype {t.dtype}", 5)
+    return table[t.dtype]
+
+
+def _code_of(dtype, like) -> int:
+    """Element code of an output dtype request (numpy or torch dtype), or of `like`."""
+    if dtype is None:
+        return _torch_code(like) if _is_tensor(like) else _NP_CODE[like.dtype]
+    if _is_tensor(like) or type(dtype).__module__.startswith("torch"):
+        torch = _torch()
+        table = {torch.uint8: U8, torch.uint16: U16, torch.int16: I16, torch.int32: I32,
+                 torch.float32: F32, torch.float64: F64}
+        if dtype in table:
+            return table[dtype]
+    return _NP_CODE[np.dtype(dtype)]
+
+
+def _dims(x):
+    if x.ndim == 2:
+        return x.shape[1], x.shape[0], 1
+    if x.ndim == 3:
+        return x.shape[1], x.shape[0], x.shape[2]
+    raise Error("ipf: image must be shaped (H, W) or (H, W, C)")
+
+
+def _view(x) -> _lib.IpfcImage:
+    """ipfc_image describing array/tensor x (rows may be pitched, samples dense)."""
+    w, h, c = _dims(x)
+    if _is_tensor(x):
+        if not x.is_cuda:
+            raise Error("ipf: torch tensors must live on a CUDA device (use numpy arrays for host images)")
+        es = x.element_size()
+        st = [s * es for s in x.stride()]
+        dense_row = (x.ndim == 2 and st[1] == es) or (x.ndim == 3 and st[2] == es and st[1] == c * es)
+        if not dense_row:
+            raise Error("ipf: image rows must be contiguous (interleaved channels)")
+        return _lib.IpfcImage(x.data_ptr(), w, h, c, _torch_code(x), st[0], MEM_DEVICE)
+    if not isinstance(x, np.ndarray):
+        raise Error("ipf: images are numpy arrays or CUDA torch tensors")
+    es = x.itemsize
+    st = x.strides
+    dense_row = (x.ndim == 2 and st[1] == es) or (x.ndim == 3 and st[2] == es and st[1] == c * es)
+    if not dense_row or st[0] < w * c * es:
+        x = np.ascontiguousarray(x)
+        st = x.strides
+    return _lib.IpfcImage(x.ctypes.data, w, h, c, _NP_CODE[x.dtype], st[0], MEM_HOST), x
+
+
+def _new_like(src, code: int):
+    if _is_tensor(src):
+        torch = _torch()
+        tmap = {U8: torch.uint8, U16: torch.uint16, I16: torch.int16, I32: torch.int32,
+                F32: torch.float32, F64: torch.float64}
+        return torch.empty(tuple(src.shape), dtype=tmap[code], device=src.device)
+    return np.empty(src.shape, _CODE_NP[code])
+
+
+def _stream_of(src, stream):
+    if stream is not None:
+        return ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    if _is_tensor(src):
+        return ctypes.c_void_p(_torch().cuda.current_stream(src.device).cuda_stream)
+    return ctypes.c_void_p(0)
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        msg = _lib.load().ipfc_last_error().decode() or f"ipf: error {rc}"
+        raise Error(msg, rc)
+
+
+def _pair(src, dtype):
+    """Returns (src view, keep-alive source, dst object, dst view)."""
+    lib = _lib.load()
+    del lib
+    if _is_tensor(src):
+        sv = _view(src)
+        keep = src
+    else:
+        sv, keep = _view(src)
+    dst = _new_like(src, _code_of(dtype, src))
+    if _is_tensor(dst):
+        dv = _view(dst)
+    else:
+        dv, dst = _view(dst)
+    return sv, keep, dst, dv
+
+
+def _f64(v) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(v, dtype=np.float64).ravel())
+
+
+# ---------------------------------------------------------------------------
+# Tap and element generators
+# ---------------------------------------------------------------------------
+
+def gaussianKernel1D(sigma: float, ksize: int = 0) -> np.ndarray:
+    """gaussianKernel1D (filter.hpp:129-145): normalised FP64 taps."""
+    lib = _lib.load()
+    buf = np.zeros(1024, np.float64)
+    n = lib.ipfc_gaussian_kernel_1d(sigma, ksize, buf.ctypes.data, buf.size)
+    if n < 0:
+        raise Error(lib.ipfc_last_error().decode())
+    if n > buf.size:
+        buf = np.zeros(n, np.float64)
+        lib.ipfc_gaussian_kernel_1d(sigma, ksize, buf.ctypes.data, buf.size)
+    return buf[:n].copy()
+
+
+def derivKernel(order: int, ksize: int) -> np.ndarray:
+    """detail::derivKernel (filter.hpp:93-114)."""
+    lib = _lib.load()
+    buf = np.zeros(64, np.float64)
+    n = lib.ipfc_deriv_kernel(order, ksize, buf.ctypes.data, buf.size)
+    if n < 0:
+        raise Error(lib.ipfc_last_error().decode())
+    return buf[:n].copy()
+
+
+def getStructuringElement(shape: int, width: int, height: int = 0) -> np.ndarray:
+    """getStructuringElement (morphology.hpp:24-49): uint8 mask shaped (h, w)."""
+    lib = _lib.load()
+    h = height if height > 0 else width
+    out = np.zeros((max(h, 0), max(width, 0)), np.uint8)
+    _check(lib.ipfc_structuring_element(int(shape), width, height, out.ctypes.data if out.size else None))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Filters
+# ---------------------------------------------------------------------------
+
+def sepFilter2D(src, kx, ky, border=BorderMode.Reflect101, delta=0.0, borderValue=0.0, dtype=None, stream=None,
+                anchor=(-1, -1)):
+    """sepFilter2D (filter.hpp:197-203) over detail::sepFilterImpl (37-90)."""
+    lib = _lib.load()
+    kx, ky = _f64(kx), _f64(ky)
+    sv, keep, dst, dv = _pair(src, dtype)
+    _check(lib.ipfc_sep_filter2d(ctypes.byref(sv), ctypes.byref(dv), kx.ctypes.data if kx.size else None, kx.size,
+                                 ky.ctypes.data if ky.size else None, ky.size, anchor[0], anchor[1], int(border),
+                                 float(delta), float(borderValue), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def gaussianBlur(src, sigmaX, sigmaY=0.0, ksize=0, border=BorderMode.Reflect101, dtype=None, stream=None):
+    """gaussianBlur (filter.hpp:262-267)."""
+    lib = _lib.load()
+    sv, keep, dst, dv = _pair(src, dtype)
+    _check(lib.ipfc_gaussian_blur(ctypes.byref(sv), ctypes.byref(dv), float(sigmaX), float(sigmaY), int(ksize),
+                                  int(border), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def boxFilter(src, kw, kh, normalize=True, border=BorderMode.Reflect101, borderValue=0.0, dtype=None, stream=None):
+    """boxFilter (filter.hpp:206-253)."""
+    lib = _lib.load()
+    sv, keep, dst, dv = _pair(src, dtype)
+    _check(lib.ipfc_box_filter(ctypes.byref(sv), ctypes.byref(dv), int(kw), int(kh), int(bool(normalize)),
+                               int(border), float(borderValue), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def blur(src, ksize, border=BorderMode.Reflect101, dtype=None, stream=None):
+    """blur (filter.hpp:256-259): normalised ksize x ksize box."""
+    return boxFilter(src, ksize, ksize, True, border, 0.0, dtype, stream)
+
+
+def sobel(src, dx, dy, ksize=3, scale=1.0, border=BorderMode.Reflect101, dtype=np.float32, stream=None):
+    """sobel (filter.hpp:395-407).  The reference returns float32; other
+    dtypes give sepFilter2D<dtype> with the same taps (e.g. int16)."""
+    lib = _lib.load()
+    sv, keep, dst, dv = _pair(src, dtype)
+    _check(lib.ipfc_sobel(ctypes.byref(sv), ctypes.byref(dv), int(dx), int(dy), int(ksize), float(scale),
+                          int(border), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def filter2D(src, kernel, border=BorderMode.Reflect101, delta=0.0, anchor=(-1, -1), borderValue=0.0, dtype=None,
+             stream=None):
+    """filter2D (filter.hpp:159-194): correlation with float32 taps (kh, kw)."""
+    lib = _lib.load()
+    k = np.ascontiguousarray(np.asarray(kernel, dtype=np.float32))
+    if k.ndim != 2 or k.size == 0:
+        raise Error("ipf: filter2D: kernel must be a non-empty single-channel image")
+    sv, keep, dst, dv = _pair(src, dtype)
+    _check(lib.ipfc_filter2d(ctypes.byref(sv), ctypes.byref(dv), k.ctypes.data, k.shape[1], k.shape[0],
+                             int(anchor[0]), int(anchor[1]), int(border), float(delta), float(borderValue),
+                             _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def medianBlur(src, ksize, border=BorderMode.Replicate, stream=None):
+    """medianBlur (filter.hpp:302-332)."""
+    lib = _lib.load()
+    sv, keep, dst, dv = _pair(src, None)
+    _check(lib.ipfc_median_blur(ctypes.byref(sv), ctypes.byref(dv), int(ksize), int(border),
+                                _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def _morph(fn, src, se, iterations, stream):
+    lib = _lib.load()
+    if se is None:
+        se = getStructuringElement(MorphShape.Rect, 3)
+    se = np.ascontiguousarray(np.asarray(se, dtype=np.uint8))
+    if se.ndim != 2 or se.size == 0:
+        raise Error("ipf: morphology: structuring element must be a non-empty single-channel mask")
+    sv, keep, dst, dv = _pair(src, None)
+    _check(getattr(lib, fn)(ctypes.byref(sv), ctypes.byref(dv), se.ctypes.data, se.shape[1], se.shape[0],
+                            int(iterations), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def erode(src, se=None, iterations=1, stream=None):
+    """erode (morphology.hpp:112-118); default element: 3x3 rect."""
+    return _morph("ipfc_erode", src, se, iterations, stream)
+
+
+def dilate(src, se=None, iterations=1, stream=None):
+    """dilate (morphology.hpp:121-127); default element: 3x3 rect."""
+    return _morph("ipfc_dilate", src, se, iterations, stream)

@@ -1,0 +1,173 @@
+/*
+ * ipfc.h -- C ABI of the B200 (sm_100a) neighbourhood-filter library.
+ *
+ * Drop-in boundary for the hot path of ImageProcessingFlex (ipf): separable
+ * correlation (sepFilter2D / gaussianBlur / boxFilter / sobel), dense
+ * filter2D, medianBlur and erode / dilate, with ipf's five BorderModes and
+ * its saturate_cast rounding.  ipf itself is header-only C++ whose "operator
+ * API" is the set of free template functions in namespace ipf; each entry
+ * point below replaces one of them and cites it as
+ * include/ipf/<file>.hpp:<line>.  The C++ wrapper include/ipf_cuda.hpp gives
+ * the same functions back as ipf::cuda::* over ipf::Image<T>.
+ *
+ * Conventions
+ *  - Images are interleaved row-major (pixel (x, y) channel c at
+ *    row(y)[x*channels + c]), like ipf::Image<T> (core.hpp:220-222).  `pitch`
+ *    is bytes between rows; 0 means dense rows.
+ *  - `mem` says where `data` lives.  IPFC_MEM_DEVICE: device pointer on the
+ *    current device; the call is asynchronous on `stream` (a cudaStream_t,
+ *    NULL = legacy default stream).  IPFC_MEM_HOST: host memory (pinned or
+ *    pageable); the call stages through device memory owned by the library
+ *    and returns after the result is back in host memory.
+ *  - dst must already have src's width, height and channel count (the
+ *    reference allocates it; here the caller does).  Its dtype selects the
+ *    output type, the TOut template argument of the reference.
+ *  - Every function returns an ipfc_status.  On failure ipfc_last_error()
+ *    returns a thread-local message; argument errors carry the reference's
+ *    own "ipf: <function>: <reason>" text (core.hpp:41-44).
+ *  - Nothing here falls back to the CPU.  With no usable CUDA device the
+ *    compute entry points fail with IPFC_ERR_CUDA.
+ */
+#ifndef IPFC_H
+#define IPFC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define IPFC_API __attribute__((visibility("default")))
+#else
+#define IPFC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Element types: the reference's ImageU8 / U16 / I16 / I32 / F / D
+ * (core.hpp:403-408). */
+typedef enum ipfc_dtype {
+    IPFC_U8 = 0,
+    IPFC_U16 = 1,
+    IPFC_I16 = 2,
+    IPFC_I32 = 3,
+    IPFC_F32 = 4,
+    IPFC_F64 = 5
+} ipfc_dtype;
+
+/* Border modes, in the order of ipf::BorderMode (core.hpp:183). */
+typedef enum ipfc_border {
+    IPFC_BORDER_CONSTANT = 0,
+    IPFC_BORDER_REPLICATE = 1,
+    IPFC_BORDER_REFLECT = 2,
+    IPFC_BORDER_REFLECT101 = 3,
+    IPFC_BORDER_WRAP = 4
+} ipfc_border;
+
+/* Structuring-element shapes, in the order of ipf::MorphShape
+ * (morphology.hpp:21). */
+typedef enum ipfc_morph_shape { IPFC_MORPH_RECT = 0, IPFC_MORPH_CROSS = 1, IPFC_MORPH_ELLIPSE = 2 } ipfc_morph_shape;
+
+typedef enum ipfc_mem { IPFC_MEM_HOST = 0, IPFC_MEM_DEVICE = 1 } ipfc_mem;
+
+typedef enum ipfc_status {
+    IPFC_OK = 0,
+    IPFC_ERR_INVALID = 1,     /* invalid argument: the reference throws ipf::Error here */
+    IPFC_ERR_NOMEM = 2,       /* device or pinned allocation failed */
+    IPFC_ERR_CUDA = 3,        /* CUDA runtime error (no device, launch failure, ...) */
+    IPFC_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+    IPFC_ERR_UNSUPPORTED = 5  /* valid for the reference, not provided by this build (dtype) */
+} ipfc_status;
+
+/* An image view.  Plain data: the library never takes ownership. */
+typedef struct ipfc_image {
+    void* data;
+    int width;
+    int height;
+    int channels;
+    int dtype;       /* ipfc_dtype */
+    long long pitch; /* bytes between row starts; 0 = width * channels * sizeof(element) */
+    int mem;         /* ipfc_mem */
+} ipfc_image;
+
+/* ---- library ------------------------------------------------------------- */
+
+/* Thread-local text of the last failure on this thread ("" when none). */
+IPFC_API const char* ipfc_last_error(void);
+
+/* (major << 16) | (minor << 8) | patch of this library. */
+IPFC_API int ipfc_version(void);
+
+/* ---- tap and element generators (host, FP64) ----------------------------- */
+
+/* gaussianKernel1D (filter.hpp:129-145).  Writes min(len, cap) taps to out and
+ * returns the kernel length, or -1 with ipfc_last_error() set. */
+IPFC_API int ipfc_gaussian_kernel_1d(double sigma, int ksize, double* out, int cap);
+
+/* detail::derivKernel (filter.hpp:93-114).  Returns the length or -1. */
+IPFC_API int ipfc_deriv_kernel(int order, int ksize, double* out, int cap);
+
+/* getStructuringElement (morphology.hpp:24-49).  out holds width*height
+ * bytes (height <= 0 means height = width). */
+IPFC_API int ipfc_structuring_element(int shape, int width, int height, uint8_t* out);
+
+/* ---- separable correlation --------------------------------------------- */
+
+/* detail::sepFilterImpl (filter.hpp:37-90), reached from sepFilter2D
+ * (filter.hpp:197-203) with anchors kw/2, kh/2.  ax/ay < 0 select those
+ * defaults.  Accumulates in FP32 on the device (FP64 on the reference). */
+IPFC_API int ipfc_sep_filter2d(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh,
+                      int ax, int ay, int border, double delta, double border_value, void* stream);
+
+/* gaussianBlur (filter.hpp:262-267): FP64 taps from gaussianKernel1D on the
+ * host, then the separable path. */
+IPFC_API int ipfc_gaussian_blur(const ipfc_image* src, ipfc_image* dst, double sigma_x, double sigma_y, int ksize, int border,
+                       void* stream);
+
+/* boxFilter (filter.hpp:206-253) and blur (filter.hpp:256-259, normalize = 1,
+ * kw = kh = ksize).  Integer sources are summed exactly. */
+IPFC_API int ipfc_box_filter(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int normalize, int border,
+                    double border_value, void* stream);
+
+/* sobel (filter.hpp:395-407).  The reference returns ImageF; any dst dtype is
+ * accepted here (IPFC_I16 gives sepFilter2D<int16_t> with the same taps). */
+IPFC_API int ipfc_sobel(const ipfc_image* src, ipfc_image* dst, int dx, int dy, int ksize, double scale, int border,
+               void* stream);
+
+/* ---- dense correlation -------------------------------------------------- */
+
+/* filter2D (filter.hpp:159-194).  kernel: kw*kh float32 taps, row-major (the
+ * reference's Kernel = ImageF).  ax/ay < 0 select kw/2, kh/2.  FP32 CUDA-core
+ * accumulation. */
+IPFC_API int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
+                  int border, double delta, double border_value, void* stream);
+
+/* ---- order statistics and morphology -------------------------------------- */
+
+/* medianBlur (filter.hpp:302-332): exact; Constant border is an error. */
+IPFC_API int ipfc_median_blur(const ipfc_image* src, ipfc_image* dst, int ksize, int border, void* stream);
+
+/* erode / dilate (morphology.hpp:112-127 over detail::morphOnce, 53-107).
+ * se: se_w*se_h mask bytes (non-zero = member), anchor (se_w/2, se_h/2).
+ * Pixels outside the image never count; there is no border mode. */
+IPFC_API int ipfc_erode(const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w, int se_h, int iterations,
+               void* stream);
+IPFC_API int ipfc_dilate(const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w, int se_h, int iterations,
+                void* stream);
+
+/* ---- device probes of the scalar rules --------------------------------- */
+
+/* borderIndex (core.hpp:187-214) evaluated by the device code the kernels
+ * use: out[i] = border index of p[i] for a row of length len.  p and out are
+ * device pointers of n ints. */
+IPFC_API int ipfc_probe_border_index(const int* p, int* out, int n, int len, int border, void* stream);
+
+/* saturate_cast<To>(float) (core.hpp:69-103) evaluated by the device store
+ * path: v is n device floats, out n elements of dtype `to`. */
+IPFC_API int ipfc_probe_saturate(const float* v, void* out, int n, int to, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IPFC_H */

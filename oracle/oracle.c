@@ -1,0 +1,497 @@
+/*
+ * oracle.c -- CPU restatement of ipf's neighbourhood-filter arithmetic.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path: it is
+ * linked by the test suite, by __graft_entry__.smoke() and by the CPU-baseline
+ * leg of bench.py, and by nothing that ships.  The product library never calls
+ * it and has no CPU fallback.
+ *
+ * Every routine restates the reference algorithm in plain C with the same
+ * floating-point operation order (FP64 accumulation, same summation order, no
+ * FMA contraction: build with -ffp-contract=off), so that its results are
+ * bit-identical to the reference's for the same inputs.  Parity is pinned two
+ * ways (tests/test_oracle_*.py): against the reference's own known-answer
+ * tests (tests/test_filter.cpp, tests/test_morphology.cpp) and against the
+ * reference headers compiled into oracle/_ref/ on many seeded inputs.
+ *
+ * Image buffers are dense, interleaved row-major (HWC), as ipf::Image<T>
+ * stores them (include/ipf/core.hpp:220-222, 389-391).
+ *
+ * Element type codes (shared with the C-ABI in include/ipfc.h):
+ *   0 u8, 1 u16, 2 i16, 3 i32, 4 f32, 5 f64.
+ * Border codes follow ipf::BorderMode's declaration order (core.hpp:183):
+ *   0 Constant, 1 Replicate, 2 Reflect, 3 Reflect101, 4 Wrap.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_U8 0
+#define ORC_U16 1
+#define ORC_I16 2
+#define ORC_I32 3
+#define ORC_F32 4
+#define ORC_F64 5
+
+#define ORC_CONSTANT 0
+#define ORC_REPLICATE 1
+#define ORC_REFLECT 2
+#define ORC_REFLECT101 3
+#define ORC_WRAP 4
+
+#define ORC_OK 0
+#define ORC_EINVAL 1
+#define ORC_ENOMEM 2
+
+/* ---------------------------------------------------------------------------
+ * Border index: include/ipf/core.hpp:187-214 (borderIndex).
+ * Maps p into [0, len) by the border rule; -1 means "use the border value".
+ * ------------------------------------------------------------------------- */
+int orc_border_index(int p, int len, int mode) {
+    if (p >= 0 && p < len) return p;
+    if (len <= 0) return -1;
+    if (mode == ORC_CONSTANT) return -1;
+    if (mode == ORC_REPLICATE) return p < 0 ? 0 : len - 1;
+    if (mode == ORC_REFLECT) {
+        long long per = 2LL * len, q = p % per;
+        if (q < 0) q += per;
+        return (int)(q < len ? q : per - 1 - q);
+    }
+    if (mode == ORC_REFLECT101) {
+        if (len == 1) return 0;
+        long long per = 2LL * len - 2, q = p % per;
+        if (q < 0) q += per;
+        return (int)(q < len ? q : per - q);
+    }
+    if (mode == ORC_WRAP) {
+        int q = p % len;
+        return q < 0 ? q + len : q;
+    }
+    return -1;
+}
+
+/* filter.hpp:28-32 (detail::borderTable): index of every padded position. */
+static int* border_table(int len, int before, int after, int mode) {
+    int n = len + before + after;
+    int* t = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    if (!t) return NULL;
+    for (int p = 0; p < n; ++p) t[p] = orc_border_index(p - before, len, mode);
+    return t;
+}
+
+/* ---------------------------------------------------------------------------
+ * Element access and saturate_cast (core.hpp:69-103).
+ * Float -> integer: NaN -> 0, d += (d < 0 ? -0.5 : 0.5) in double, saturate
+ * at the type's limits, then truncate.  Float -> float: plain conversion.
+ * ------------------------------------------------------------------------- */
+static double load_elem(const void* p, int dt, size_t i) {
+    switch (dt) {
+        case ORC_U8: return (double)((const uint8_t*)p)[i];
+        case ORC_U16: return (double)((const uint16_t*)p)[i];
+        case ORC_I16: return (double)((const int16_t*)p)[i];
+        case ORC_I32: return (double)((const int32_t*)p)[i];
+        case ORC_F32: return (double)((const float*)p)[i];
+        default: return ((const double*)p)[i];
+    }
+}
+
+static void range_of(int dt, double* lo, double* hi) {
+    switch (dt) {
+        case ORC_U8: *lo = 0; *hi = 255; break;
+        case ORC_U16: *lo = 0; *hi = 65535; break;
+        case ORC_I16: *lo = -32768; *hi = 32767; break;
+        default: *lo = -2147483648.0; *hi = 2147483647.0; break;
+    }
+}
+
+static void store_sat(void* p, int dt, size_t i, double v) {
+    if (dt == ORC_F32) { ((float*)p)[i] = (float)v; return; }
+    if (dt == ORC_F64) { ((double*)p)[i] = v; return; }
+    double lo, hi;
+    range_of(dt, &lo, &hi);
+    long long r;
+    if (!(v == v)) {
+        r = 0;
+    } else {
+        double d = v < 0 ? v - 0.5 : v + 0.5;
+        if (d <= lo) r = (long long)lo;
+        else if (d >= hi) r = (long long)hi;
+        else r = (long long)d; /* truncation toward zero */
+    }
+    switch (dt) {
+        case ORC_U8: ((uint8_t*)p)[i] = (uint8_t)r; break;
+        case ORC_U16: ((uint16_t*)p)[i] = (uint16_t)r; break;
+        case ORC_I16: ((int16_t*)p)[i] = (int16_t)r; break;
+        default: ((int32_t*)p)[i] = (int32_t)r; break;
+    }
+}
+
+/* Same-type copy used where the reference returns the source unchanged. */
+static size_t elem_size(int dt) {
+    static const size_t sz[] = {1, 2, 2, 4, 4, 8};
+    return (dt >= 0 && dt <= 5) ? sz[dt] : 0;
+}
+
+double orc_saturate(double v, int dt) {
+    /* Scalar probe of the cast above, for the tests. */
+    union { uint8_t u8; uint16_t u16; int16_t i16; int32_t i32; float f; double d; } u;
+    store_sat(&u, dt, 0, v);
+    return load_elem(&u, dt, 0);
+}
+
+/* ---------------------------------------------------------------------------
+ * Tap generators.
+ * ------------------------------------------------------------------------- */
+
+/* filter.hpp:129-145 (gaussianKernel1D).  Writes up to cap taps; returns the
+ * kernel length, or -1 for invalid arguments. */
+int orc_gaussian_kernel_1d(double sigma, int ksize, double* out, int cap) {
+    if (ksize <= 0) {
+        if (!(sigma > 0)) return -1;
+        int r = (int)(3.0 * sigma + 0.5);
+        ksize = 2 * (r > 1 ? r : 1) + 1;
+    }
+    if (ksize % 2 != 1) return -1;
+    if (sigma <= 0) sigma = 0.3 * ((ksize - 1) * 0.5 - 1) + 0.8;
+    if (ksize > cap) return ksize; /* caller retries with room */
+    const int c = ksize / 2;
+    double sum = 0;
+    for (int i = 0; i < ksize; ++i) {
+        out[i] = exp(-0.5 * (i - c) * (i - c) / (sigma * sigma));
+        sum += out[i];
+    }
+    for (int i = 0; i < ksize; ++i) out[i] /= sum;
+    return ksize;
+}
+
+/* filter.hpp:93-114 (detail::derivKernel): binomial smoothing convolved with
+ * (-1, 1) `order` times.  Returns the length or -1. */
+int orc_deriv_kernel(int order, int ksize, double* out, int cap) {
+    if (ksize == 1) {
+        if (cap < 3) return -1;
+        if (order == 0) { out[0] = 1; return 1; }
+        if (order == 1) { out[0] = -1; out[1] = 0; out[2] = 1; return 3; }
+        if (order == 2) { out[0] = 1; out[1] = -2; out[2] = 1; return 3; }
+        return -1;
+    }
+    if (ksize % 2 != 1 || ksize < 3 || ksize > 31) return -1;
+    if (order < 0 || order >= ksize || cap < ksize) return -1;
+    double k[32], r[32];
+    int n = 1;
+    k[0] = 1.0;
+    for (int step = 0; step < ksize - 1; ++step) {
+        const double a = step < ksize - 1 - order ? 1.0 : -1.0, b = 1.0;
+        for (int i = 0; i <= n; ++i) r[i] = 0.0;
+        for (int i = 0; i < n; ++i) {
+            r[i] += k[i] * a;
+            r[i + 1] += k[i] * b;
+        }
+        ++n;
+        for (int i = 0; i < n; ++i) k[i] = r[i];
+    }
+    for (int i = 0; i < n; ++i) out[i] = k[i];
+    return n;
+}
+
+/* morphology.hpp:24-49 (getStructuringElement): 0 Rect, 1 Cross, 2 Ellipse. */
+int orc_structuring_element(int shape, int width, int height, uint8_t* out) {
+    if (height <= 0) height = width;
+    if (width <= 0 || height <= 0) return ORC_EINVAL;
+    memset(out, 0, (size_t)width * height);
+    const int r = height / 2, c = width / 2;
+    const double inv_r2 = r ? 1.0 / ((double)r * r) : 0.0;
+    for (int i = 0; i < height; ++i) {
+        int j1 = 0, j2 = 0;
+        if (shape == 0 || (shape == 1 && i == r)) {
+            j1 = 0;
+            j2 = width;
+        } else if (shape == 1) {
+            j1 = c;
+            j2 = c + 1;
+        } else {
+            const int dy = i - r;
+            if (abs(dy) <= r) {
+                /* saturate_cast<int>(double): round half away from zero */
+                const double v = c * sqrt((r * r - dy * dy) * inv_r2);
+                const int dx = (int)(v + 0.5);
+                j1 = c - dx > 0 ? c - dx : 0;
+                j2 = c + dx + 1 < width ? c + dx + 1 : width;
+            }
+        }
+        for (int j = j1; j < j2; ++j) out[(size_t)i * width + j] = 1;
+    }
+    return ORC_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Separable correlation: filter.hpp:37-90 (detail::sepFilterImpl).
+ * Pass 1 fills an FP64 intermediate of (H + kh - 1) padded rows, each the
+ * horizontal correlation of a border-extended source row, accumulated tap by
+ * tap from 0.0.  Pass 2 starts every output at delta, adds the vertical taps
+ * in order, and saturates to the output type.
+ * ------------------------------------------------------------------------- */
+int orc_sep_filter(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, const double* kx, int kw,
+                   const double* ky, int kh, int ax, int ay, int border, double delta, double border_value) {
+    if (kw <= 0 || kh <= 0) return ORC_EINVAL;
+    if (W <= 0 || H <= 0) return ORC_OK;
+    int* xt = border_table(W, ax, kw - 1 - ax, border);
+    int* yt = border_table(H, ay, kh - 1 - ay, border);
+    const int PH = H + kh - 1, PW = W + kw - 1;
+    const size_t row = (size_t)W * C;
+    double* tmp = (double*)malloc(sizeof(double) * (size_t)PH * row);
+    double* pad = (double*)malloc(sizeof(double) * (size_t)PW * C);
+    double* acc = (double*)malloc(sizeof(double) * row);
+    if (!xt || !yt || !tmp || !pad || !acc) {
+        free(xt); free(yt); free(tmp); free(pad); free(acc);
+        return ORC_ENOMEM;
+    }
+    for (int py = 0; py < PH; ++py) {
+        const int sy = yt[py];
+        for (int px = 0; px < PW; ++px)
+            for (int c = 0; c < C; ++c)
+                pad[(size_t)px * C + c] = (sy < 0 || xt[px] < 0)
+                                              ? border_value
+                                              : load_elem(src, sdt, ((size_t)sy * W + xt[px]) * C + c);
+        double* t = tmp + (size_t)py * row;
+        for (size_t q = 0; q < row; ++q) t[q] = 0.0;
+        for (int i = 0; i < kw; ++i) {
+            const double k = kx[i];
+            const double* b = pad + (size_t)i * C;
+            for (size_t q = 0; q < row; ++q) t[q] += k * b[q];
+        }
+    }
+    for (int y = 0; y < H; ++y) {
+        for (size_t q = 0; q < row; ++q) acc[q] = delta;
+        for (int j = 0; j < kh; ++j) {
+            const double k = ky[j];
+            const double* r = tmp + (size_t)(y + j) * row;
+            for (size_t q = 0; q < row; ++q) acc[q] += k * r[q];
+        }
+        for (size_t q = 0; q < row; ++q) store_sat(dst, ddt, (size_t)y * row + q, acc[q]);
+    }
+    free(xt); free(yt); free(tmp); free(pad); free(acc);
+    return ORC_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Dense correlation: filter.hpp:159-194 (filter2D).  Taps are float32; zero
+ * taps are dropped; each sample starts at delta and adds the remaining taps in
+ * row-major order in FP64, then saturates.
+ * ------------------------------------------------------------------------- */
+int orc_filter2d(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, const float* kernel, int kw, int kh,
+                 int ax, int ay, int border, double delta, double border_value) {
+    if (kw <= 0 || kh <= 0) return ORC_EINVAL;
+    if (ax < 0) ax = kw / 2;
+    if (ay < 0) ay = kh / 2;
+    if (ax >= kw || ay >= kh) return ORC_EINVAL;
+    if (W <= 0 || H <= 0) return ORC_OK;
+    int ntap = 0;
+    int* tdx = (int*)malloc(sizeof(int) * (size_t)kw * kh);
+    int* tdy = (int*)malloc(sizeof(int) * (size_t)kw * kh);
+    double* tw = (double*)malloc(sizeof(double) * (size_t)kw * kh);
+    int* xt = border_table(W, ax, kw - 1 - ax, border);
+    int* yt = border_table(H, ay, kh - 1 - ay, border);
+    if (!tdx || !tdy || !tw || !xt || !yt) {
+        free(tdx); free(tdy); free(tw); free(xt); free(yt);
+        return ORC_ENOMEM;
+    }
+    for (int j = 0; j < kh; ++j)
+        for (int i = 0; i < kw; ++i) {
+            const float w = kernel[(size_t)j * kw + i];
+            if (w != 0.f) {
+                tdx[ntap] = i;
+                tdy[ntap] = j;
+                tw[ntap] = (double)w;
+                ++ntap;
+            }
+        }
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+            for (int c = 0; c < C; ++c) {
+                double s = delta;
+                for (int t = 0; t < ntap; ++t) {
+                    const int sx = xt[x + tdx[t]], sy = yt[y + tdy[t]];
+                    s += tw[t] * ((sx < 0 || sy < 0) ? border_value
+                                                     : load_elem(src, sdt, ((size_t)sy * W + sx) * C + c));
+                }
+                store_sat(dst, ddt, ((size_t)y * W + x) * C + c, s);
+            }
+    free(tdx); free(tdy); free(tw); free(xt); free(yt);
+    return ORC_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Box filter: filter.hpp:206-253 (boxFilter).  Horizontal window sums by a
+ * running add/subtract per padded row, then vertical running column sums,
+ * each output = column sum * (normalize ? 1/(kw*kh) : 1), saturated.
+ * Anchor at (kw/2, kh/2), also for even sizes.
+ * ------------------------------------------------------------------------- */
+int orc_box_filter(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, int kw, int kh, int normalize,
+                   int border, double border_value) {
+    if (kw <= 0 || kh <= 0) return ORC_EINVAL;
+    if (W <= 0 || H <= 0) return ORC_OK;
+    const int ax = kw / 2, ay = kh / 2;
+    int* xt = border_table(W, ax, kw - 1 - ax, border);
+    int* yt = border_table(H, ay, kh - 1 - ay, border);
+    const int PH = H + kh - 1;
+    const size_t row = (size_t)W * C;
+    double* rows = (double*)malloc(sizeof(double) * (size_t)PH * row);
+    double* col = (double*)malloc(sizeof(double) * row);
+    if (!xt || !yt || !rows || !col) {
+        free(xt); free(yt); free(rows); free(col);
+        return ORC_ENOMEM;
+    }
+    for (int py = 0; py < PH; ++py) {
+        const int sy = yt[py];
+        double* r = rows + (size_t)py * row;
+        for (int c = 0; c < C; ++c) {
+#define BOXVAL(px) ((sy < 0 || xt[(px)] < 0) ? border_value : load_elem(src, sdt, ((size_t)sy * W + xt[(px)]) * C + c))
+            double s = 0;
+            for (int i = 0; i < kw; ++i) s += BOXVAL(i);
+            r[c] = s;
+            for (int x = 1; x < W; ++x) {
+                s += BOXVAL(x + kw - 1) - BOXVAL(x - 1);
+                r[(size_t)x * C + c] = s;
+            }
+#undef BOXVAL
+        }
+    }
+    const double scale = normalize ? 1.0 / ((double)kw * kh) : 1.0;
+    for (size_t q = 0; q < row; ++q) {
+        double s = 0.0;
+        for (int j = 0; j < kh; ++j) s += rows[(size_t)j * row + q];
+        col[q] = s;
+    }
+    for (int y = 0; y < H; ++y) {
+        for (size_t q = 0; q < row; ++q) store_sat(dst, ddt, (size_t)y * row + q, col[q] * scale);
+        if (y + 1 < H)
+            for (size_t q = 0; q < row; ++q)
+                col[q] += rows[(size_t)(y + kh) * row + q] - rows[(size_t)y * row + q];
+    }
+    free(xt); free(yt); free(rows); free(col);
+    return ORC_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Median: filter.hpp:302-332 (medianBlur) and 271-297 (Huang histogram path).
+ * Both reference paths return the value of rank k*k/2 of the window, so one
+ * selection routine restates both.  Constant border is an error; ksize 1 and
+ * empty images return the source.
+ * ------------------------------------------------------------------------- */
+static int cmp_double(const void* a, const void* b) {
+    const double x = *(const double*)a, y = *(const double*)b;
+    return (x > y) - (x < y);
+}
+
+int orc_median_blur(const void* src, int dt, int W, int H, int C, void* dst, int ksize, int border) {
+    if (ksize < 1 || ksize % 2 != 1) return ORC_EINVAL;
+    if (border == ORC_CONSTANT) return ORC_EINVAL;
+    const size_t total = (size_t)W * H * C;
+    if (W <= 0 || H <= 0) return ORC_OK;
+    if (ksize == 1) {
+        memcpy(dst, src, total * elem_size(dt));
+        return ORC_OK;
+    }
+    const int r = ksize / 2;
+    int* xt = border_table(W, r, r, border);
+    int* yt = border_table(H, r, r, border);
+    const size_t n = (size_t)ksize * ksize;
+    double* win = (double*)malloc(sizeof(double) * n);
+    if (!xt || !yt || !win) {
+        free(xt); free(yt); free(win);
+        return ORC_ENOMEM;
+    }
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+            for (int c = 0; c < C; ++c) {
+                size_t k = 0;
+                for (int j = 0; j < ksize; ++j)
+                    for (int i = 0; i < ksize; ++i)
+                        win[k++] = load_elem(src, dt, ((size_t)yt[y + j] * W + xt[x + i]) * C + c);
+                qsort(win, n, sizeof(double), cmp_double);
+                store_sat(dst, dt, ((size_t)y * W + x) * C + c, win[n / 2]);
+            }
+    free(xt); free(yt); free(win);
+    return ORC_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Erosion / dilation: morphology.hpp:53-107 (detail::morphOnce), 112-127.
+ * An all-ones element runs as a row pass then a column pass over windows
+ * clipped to the image; any other element visits its offsets, skipping those
+ * outside the image, starting from the centre sample and replacing it with
+ * the first in-image value.  No border mode: outside pixels never count.
+ * ------------------------------------------------------------------------- */
+static void morph_once(const double* s, double* d, double* tmp, int W, int H, int C, const uint8_t* se, int sw,
+                       int sh, int is_min) {
+    const int ax = sw / 2, ay = sh / 2;
+    int is_rect = 1;
+    for (int i = 0; i < sw * sh; ++i)
+        if (!se[i]) is_rect = 0;
+#define BETTER(a, b) (is_min ? ((a) < (b)) : ((b) < (a)))
+#define AT(buf, x, y, c) (buf)[((size_t)(y) * W + (x)) * C + (c)]
+    if (is_rect) {
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x)
+                for (int c = 0; c < C; ++c) {
+                    double v = AT(s, x, y, c);
+                    const int i0 = x - ax > 0 ? x - ax : 0, i1 = x - ax + sw - 1 < W - 1 ? x - ax + sw - 1 : W - 1;
+                    for (int i = i0; i <= i1; ++i)
+                        if (BETTER(AT(s, i, y, c), v)) v = AT(s, i, y, c);
+                    AT(tmp, x, y, c) = v;
+                }
+        for (int y = 0; y < H; ++y)
+            for (int x = 0; x < W; ++x)
+                for (int c = 0; c < C; ++c) {
+                    double v = AT(tmp, x, y, c);
+                    const int j0 = y - ay > 0 ? y - ay : 0, j1 = y - ay + sh - 1 < H - 1 ? y - ay + sh - 1 : H - 1;
+                    for (int j = j0; j <= j1; ++j)
+                        if (BETTER(AT(tmp, x, j, c), v)) v = AT(tmp, x, j, c);
+                    AT(d, x, y, c) = v;
+                }
+        return;
+    }
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+            for (int c = 0; c < C; ++c) {
+                int any = 0;
+                double v = AT(s, x, y, c);
+                for (int j = 0; j < sh; ++j)
+                    for (int i = 0; i < sw; ++i) {
+                        if (!se[(size_t)j * sw + i]) continue;
+                        const int sx = x + i - ax, sy = y + j - ay;
+                        if (sx < 0 || sy < 0 || sx >= W || sy >= H) continue;
+                        const double sv = AT(s, sx, sy, c);
+                        if (!any || BETTER(sv, v)) v = sv;
+                        any = 1;
+                    }
+                AT(d, x, y, c) = v;
+            }
+#undef AT
+#undef BETTER
+}
+
+int orc_morph(const void* src, int dt, int W, int H, int C, void* dst, const uint8_t* se, int sw, int sh, int is_erode,
+              int iterations) {
+    if (sw <= 0 || sh <= 0) return ORC_EINVAL;
+    const size_t total = (size_t)W * H * C;
+    if (total == 0) return ORC_OK;
+    double* a = (double*)malloc(sizeof(double) * total);
+    double* b = (double*)malloc(sizeof(double) * total);
+    double* t = (double*)malloc(sizeof(double) * total);
+    if (!a || !b || !t) {
+        free(a); free(b); free(t);
+        return ORC_ENOMEM;
+    }
+    for (size_t i = 0; i < total; ++i) a[i] = load_elem(src, dt, i);
+    for (int it = 0; it < iterations; ++it) {
+        morph_once(a, b, t, W, H, C, se, sw, sh, is_erode);
+        double* sw_ = a;
+        a = b;
+        b = sw_;
+    }
+    for (size_t i = 0; i < total; ++i) store_sat(dst, dt, i, a[i]);
+    free(a); free(b); free(t);
+    return ORC_OK;
+}

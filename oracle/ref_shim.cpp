@@ -1,0 +1,195 @@
+// ref_shim.cpp -- C entry points over the reference's own headers.
+//
+// TEST INFRASTRUCTURE ONLY.  Compiled by oracle/Makefile against the reference
+// headers where they lie (include/ipf/*.hpp of ImageProcessingFlex) into
+// oracle/_ref/libipfref.so.  It is used to pin the C restatement in
+// oracle/oracle.c against the reference itself, to generate the golden
+// fixtures under tests/golden/, and as the timed CPU baseline (the reference's
+// threaded CPU path, ipf::setNumThreads(0)).  Nothing that ships links it.
+//
+// Signatures mirror oracle.c's orc_* functions with a ref_ prefix; element and
+// border codes are the same.
+#include <ipf/filter.hpp>
+#include <ipf/morphology.hpp>
+
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+using namespace ipf;
+
+template <class T>
+Image<T> wrap(const void* p, int W, int H, int C) {
+    return Image<T>::fromData(W, H, C, static_cast<const T*>(p));
+}
+
+template <class T>
+void unwrap(const Image<T>& img, void* out) {
+    if (!img.empty()) std::memcpy(out, img.data(), img.sampleCount() * sizeof(T));
+}
+
+// Calls fn.template operator()<T>() with T the element type of code dt.
+template <class Fn>
+int dispatch(int dt, Fn&& fn) {
+    switch (dt) {
+        case 0: fn(std::uint8_t{}); return 0;
+        case 1: fn(std::uint16_t{}); return 0;
+        case 2: fn(std::int16_t{}); return 0;
+        case 3: fn(std::int32_t{}); return 0;
+        case 4: fn(float{}); return 0;
+        case 5: fn(double{}); return 0;
+        default: return 1;
+    }
+}
+
+int guard(const std::function<int()>& f) {
+    try {
+        return f();
+    } catch (const ipf::Error&) {
+        return 1;
+    } catch (...) {
+        return 2;
+    }
+}
+
+BorderMode bm(int b) { return static_cast<BorderMode>(b); }
+
+}  // namespace
+
+extern "C" {
+
+void ref_set_threads(int n) { ipf::setNumThreads(n); }
+int ref_get_threads(void) { return ipf::getNumThreads(); }
+
+int ref_gaussian_kernel_1d(double sigma, int ksize, double* out, int cap) {
+    try {
+        const std::vector<double> k = ipf::gaussianKernel1D(sigma, ksize);
+        if (static_cast<int>(k.size()) <= cap) std::memcpy(out, k.data(), k.size() * sizeof(double));
+        return static_cast<int>(k.size());
+    } catch (...) {
+        return -1;
+    }
+}
+
+int ref_deriv_kernel(int order, int ksize, double* out, int cap) {
+    try {
+        const std::vector<double> k = ipf::detail::derivKernel(order, ksize);
+        if (static_cast<int>(k.size()) > cap) return -1;
+        std::memcpy(out, k.data(), k.size() * sizeof(double));
+        return static_cast<int>(k.size());
+    } catch (...) {
+        return -1;
+    }
+}
+
+int ref_structuring_element(int shape, int w, int h, std::uint8_t* out) {
+    return guard([&] {
+        const auto se = ipf::getStructuringElement(static_cast<MorphShape>(shape), w, h);
+        std::memcpy(out, se.data(), se.sampleCount());
+        return 0;
+    });
+}
+
+int ref_sep_filter(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, const double* kx, int kw,
+                   const double* ky, int kh, int ax, int ay, int border, double delta, double bv) {
+    return guard([&] {
+        std::vector<double> vx(kx, kx + kw), vy(ky, ky + kh);
+        int rc = 0;
+        dispatch(sdt, [&](auto s) {
+            using S = decltype(s);
+            const Image<S> in = wrap<S>(src, W, H, C);
+            rc = dispatch(ddt, [&](auto d) {
+                using D = decltype(d);
+                unwrap(detail::sepFilterImpl<D>(in, vx, vy, ax, ay, bm(border), delta, bv), dst);
+            });
+        });
+        return rc;
+    });
+}
+
+int ref_gaussian_blur(const void* src, int dt, int W, int H, int C, void* dst, int ddt, double sx, double sy,
+                      int ksize, int border) {
+    return guard([&] {
+        int rc = 0;
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            const Image<S> in = wrap<S>(src, W, H, C);
+            rc = dispatch(ddt, [&](auto d) {
+                using D = decltype(d);
+                unwrap(ipf::gaussianBlur<D>(in, sx, sy, ksize, bm(border)), dst);
+            });
+        });
+        return rc;
+    });
+}
+
+int ref_filter2d(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, const float* k, int kw, int kh,
+                 int ax, int ay, int border, double delta, double bv) {
+    return guard([&] {
+        const Kernel kern = Kernel::fromData(kw, kh, 1, k);
+        int rc = 0;
+        dispatch(sdt, [&](auto s) {
+            using S = decltype(s);
+            const Image<S> in = wrap<S>(src, W, H, C);
+            rc = dispatch(ddt, [&](auto d) {
+                using D = decltype(d);
+                unwrap(ipf::filter2D<D>(in, kern, bm(border), delta, Point(ax, ay), bv), dst);
+            });
+        });
+        return rc;
+    });
+}
+
+int ref_box_filter(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, int kw, int kh, int normalize,
+                   int border, double bv) {
+    return guard([&] {
+        int rc = 0;
+        dispatch(sdt, [&](auto s) {
+            using S = decltype(s);
+            const Image<S> in = wrap<S>(src, W, H, C);
+            rc = dispatch(ddt, [&](auto d) {
+                using D = decltype(d);
+                unwrap(ipf::boxFilter<D>(in, kw, kh, normalize != 0, bm(border), bv), dst);
+            });
+        });
+        return rc;
+    });
+}
+
+int ref_sobel(const void* src, int sdt, int W, int H, int C, float* dst, int dx, int dy, int ksize, double scale,
+              int border) {
+    return guard([&] {
+        dispatch(sdt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::sobel(wrap<S>(src, W, H, C), dx, dy, ksize, scale, bm(border)), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_median_blur(const void* src, int dt, int W, int H, int C, void* dst, int ksize, int border) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::medianBlur(wrap<S>(src, W, H, C), ksize, bm(border)), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_morph(const void* src, int dt, int W, int H, int C, void* dst, const std::uint8_t* se, int sw, int sh,
+              int is_erode, int iterations) {
+    return guard([&] {
+        const StructuringElement el = StructuringElement::fromData(sw, sh, 1, se);
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            const Image<S> in = wrap<S>(src, W, H, C);
+            unwrap(is_erode ? ipf::erode(in, el, iterations) : ipf::dilate(in, el, iterations), dst);
+        });
+        return 0;
+    });
+}
+
+}  // extern "C"

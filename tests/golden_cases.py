@@ -1,0 +1,141 @@
+"""Loads the golden fixtures (tests/golden/, made by make_golden.py from the
+reference's compiled headers) and replays a case through a backend.
+
+Backends: the C restatement (``oracle.restatement()``) and the CUDA path
+(``imageprocessingflex_b200``).  Both are driven through the same
+``run_case`` so a case means the same call everywhere.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+
+_cache = {}
+
+
+def load():
+    if "cases" not in _cache:
+        with open(os.path.join(GOLDEN, "cases.json")) as f:
+            _cache["cases"] = json.load(f)
+        _cache["arrays"] = np.load(os.path.join(GOLDEN, "arrays.npz"))
+    return _cache["cases"], _cache["arrays"]
+
+
+def case_ids():
+    cases, _ = load()
+    return [f"{i}-{c['op']}" for i, c in enumerate(cases)]
+
+
+def case(i):
+    cases, arrays = load()
+    c = cases[i]
+    inputs = {k: arrays[v] for k, v in c["inputs"].items()}
+    return c["op"], c["params"], inputs, arrays[c["out"]]
+
+
+def run_oracle(orc, op, p, x):
+    dt = np.dtype(p["dtype"]) if "dtype" in p else None
+    if op == "gaussian":
+        return orc.gaussian_blur(x["src"], p["sigma_x"], p["sigma_y"], p["ksize"], p["border"], dt)
+    if op == "sep":
+        return orc.sep_filter(x["src"], x["kx"], x["ky"], border=p["border"], delta=p["delta"],
+                              border_value=p["border_value"], out_dtype=dt)
+    if op == "sobel":
+        return orc.sobel(x["src"], p["dx"], p["dy"], p["ksize"], p["scale"], p["border"])
+    if op == "box":
+        return orc.box_filter(x["src"], p["kw"], p["kh"], p["normalize"], p["border"], p["border_value"], dt)
+    if op == "filter2d":
+        return orc.filter2d(x["src"], x["kernel"], p["border"], p["delta"], tuple(p["anchor"]), p["border_value"])
+    if op == "median":
+        return orc.median_blur(x["src"], p["ksize"], p["border"])
+    if op == "erode":
+        return orc.erode(x["src"], x["se"], p["iterations"])
+    if op == "dilate":
+        return orc.dilate(x["src"], x["se"], p["iterations"])
+    raise KeyError(op)
+
+
+def run_gpu(ipf, op, p, x, device_images=False):
+    """Runs a case through the CUDA library; host arrays by default, or CUDA
+    tensors (device-resident path) when device_images is set."""
+    src = x["src"]
+    if device_images:
+        import torch
+
+        src = torch.from_numpy(np.ascontiguousarray(src)).cuda()
+    dt = np.dtype(p["dtype"]) if "dtype" in p else None
+    if dt is not None and device_images:
+        import torch
+
+        dt = {np.dtype(np.float32): torch.float32, np.dtype(np.int16): torch.int16,
+              np.dtype(np.uint8): torch.uint8}[dt]
+    B = ipf.BorderMode
+    if op == "gaussian":
+        out = ipf.gaussianBlur(src, p["sigma_x"], p["sigma_y"], p["ksize"], B(p["border"]), dtype=dt)
+    elif op == "sep":
+        out = ipf.sepFilter2D(src, x["kx"], x["ky"], B(p["border"]), p["delta"], p["border_value"], dtype=dt)
+    elif op == "sobel":
+        out = ipf.sobel(src, p["dx"], p["dy"], p["ksize"], p["scale"], B(p["border"]))
+    elif op == "box":
+        out = ipf.boxFilter(src, p["kw"], p["kh"], p["normalize"], B(p["border"]), p["border_value"], dtype=dt)
+    elif op == "filter2d":
+        out = ipf.filter2D(src, x["kernel"], B(p["border"]), p["delta"], tuple(p["anchor"]), p["border_value"])
+    elif op == "median":
+        out = ipf.medianBlur(src, p["ksize"], B(p["border"]))
+    elif op == "erode":
+        out = ipf.erode(src, x["se"], p["iterations"])
+    elif op == "dilate":
+        out = ipf.dilate(src, x["se"], p["iterations"])
+    else:
+        raise KeyError(op)
+    if device_images:
+        out = out.cpu().numpy()
+    return out
+
+
+def tolerance(op, p, x, want):
+    """(kind, value) of the parity bar for a GPU result against the reference.
+
+    exact  -- integer arithmetic: median, morphology, box on integer sources,
+              Sobel and other integer-tap separable filters on integer sources
+              whose sums stay below 2^24 (exact in FP32);
+    lsb    -- integer destination of an FP32-accumulated sum: within 1;
+    rel    -- float destination: |d| <= tol * max(1, |ref|) with tol 1e-5
+              (2e-5 for filter2D, whose taps may sum to large magnitudes).
+    """
+    if op in ("median", "erode", "dilate"):
+        return ("exact", 0)
+    if op == "box" and x["src"].dtype != np.float32:
+        return ("exact", 0)
+    if op in ("sep", "sobel") and x["src"].dtype != np.float32:
+        kx = x.get("kx")
+        ky = x.get("ky")
+        if kx is not None and np.all(kx == np.round(kx)) and np.all(ky == np.round(ky)):
+            return ("exact", 0)
+        if op == "sobel":
+            return ("exact", 0)
+    if want.dtype.kind in "iu":
+        return ("lsb", 1)
+    return ("rel", 2e-5 if op == "filter2d" else 1e-5)
+
+
+def compare(got, want, tol):
+    kind, v = tol
+    assert got.shape == want.shape and got.dtype == want.dtype, (got.shape, got.dtype, want.shape, want.dtype)
+    if kind == "exact":
+        bad = np.flatnonzero(got != want)
+        assert bad.size == 0, f"{bad.size} mismatches, first at {bad[:5]}: got {got.ravel()[bad[:5]]} want " \
+                              f"{want.ravel()[bad[:5]]}"
+        return 0
+    d = np.abs(got.astype(np.float64) - want.astype(np.float64))
+    if kind == "lsb":
+        assert d.max(initial=0) <= v, f"max |diff| {d.max()} > {v} LSB"
+        return int((d > 0).sum())
+    lim = v * np.maximum(1.0, np.abs(want.astype(np.float64)))
+    assert np.all(d <= lim), f"max |diff| {d.max()} exceeds {v} x max(1, |ref|)"
+    return 0

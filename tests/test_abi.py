@@ -1,0 +1,102 @@
+"""The C-ABI library: loads, exports every symbol include/*.h declares, checks
+arguments with the reference's messages, and never computes on the CPU.
+
+No compute call here reaches a GPU; the device-independent parts (argument
+checks, FP64 tap generators) run on any machine.
+"""
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+import imageprocessingflex_b200 as ipf
+from imageprocessingflex_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        with open(h) as f:
+            text = f.read()
+        names.update(re.findall(r"IPFC_API\s+[\w\s\*]*?\b(ipfc_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.library_path() if os.path.exists(_lib.library_path()) else _lib.load()._name)
+    names = declared_symbols()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python binding describes each of them
+    bound = set(_lib.exported_names())
+    assert set(names) <= bound, sorted(set(names) - bound)
+
+
+def test_version():
+    assert _lib.load().ipfc_version() >> 16 == 1
+
+
+def test_tap_generators_match_restatement(orc):
+    for s in (0.5, 1.0, 2.0, 2.3, 4.0):
+        np.testing.assert_array_equal(ipf.gaussianKernel1D(s), orc.gaussian_kernel_1d(s))
+    np.testing.assert_array_equal(ipf.gaussianKernel1D(0, 7), orc.gaussian_kernel_1d(0, 7))
+    for order, k in ((1, 3), (1, 5), (2, 5), (0, 7), (1, 1), (2, 1), (3, 31)):
+        np.testing.assert_array_equal(ipf.derivKernel(order, k), orc.deriv_kernel(order, k))
+    for shape in (0, 1, 2):
+        for w, h in ((3, 3), (5, 7), (9, 5), (1, 1), (4, 2)):
+            np.testing.assert_array_equal(ipf.getStructuringElement(shape, w, h), orc.structuring_element(shape, w, h))
+
+
+@pytest.mark.parametrize("call, msg", [
+    (lambda x: ipf.medianBlur(x, 4), "ipf: medianBlur: ksize must be odd and positive"),
+    (lambda x: ipf.medianBlur(x, 3, ipf.BorderMode.Constant), "ipf: medianBlur: Constant border is not supported"),
+    (lambda x: ipf.sepFilter2D(x, [], [1.0]), "ipf: separable filter: empty kernel"),
+    (lambda x: ipf.boxFilter(x, 0, 3), "ipf: boxFilter: kernel size must be positive"),
+    (lambda x: ipf.gaussianBlur(x, 0.0), "ipf: gaussianKernel1D: need sigma > 0 or ksize > 0"),
+    (lambda x: ipf.gaussianBlur(x, 1.0, 0.0, 4), "ipf: gaussianKernel1D: ksize must be odd"),
+    (lambda x: ipf.sobel(x, 0, 0), "ipf: sobel: need dx + dy > 0"),
+    (lambda x: ipf.sobel(x, 1, 0, 4), "ipf: derivKernel: ksize must be odd in [3, 31]"),
+    (lambda x: ipf.filter2D(x, np.ones((3, 3)), anchor=(3, 0)), "ipf: filter2D: anchor outside kernel"),
+    (lambda x: ipf.filter2D(x, np.ones((0, 3))), "ipf: filter2D: kernel must be a non-empty single-channel image"),
+    (lambda x: ipf.erode(x, np.ones((0, 0))),
+     "ipf: morphology: structuring element must be a non-empty single-channel mask"),
+])
+def test_argument_errors_carry_reference_messages(call, msg):
+    x = np.zeros((8, 8), np.uint8)
+    with pytest.raises(ipf.Error) as e:
+        call(x)
+    assert str(e.value) == msg
+    assert e.value.status == 1
+
+
+def test_structuring_element_error():
+    with pytest.raises(ipf.Error, match="ipf: getStructuringElement: size must be positive"):
+        ipf.getStructuringElement(ipf.MorphShape.Rect, 0)
+
+
+def test_unsupported_dtype_is_reported_not_emulated():
+    with pytest.raises(ipf.Error) as e:
+        ipf.gaussianBlur(np.zeros((4, 4), np.float64), 1.0)
+    assert e.value.status == 5
+
+
+def test_empty_image_returns_empty():
+    out = ipf.gaussianBlur(np.zeros((0, 5, 3), np.uint8), 2.0)
+    assert out.shape == (0, 5, 3)
+
+
+def test_no_cpu_fallback_without_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(ipf.Error) as e:
+        ipf.gaussianBlur(np.zeros((4, 4), np.uint8), 1.0)
+    assert e.value.status == 3
+    assert "no CUDA device" in str(e.value)

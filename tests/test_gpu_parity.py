@@ -1,0 +1,225 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Every golden fixture -- outputs of the reference's own compiled headers -- is
+replayed through the CUDA library from host arrays, and a subset from device
+tensors; seeded random cases, edge shapes and full-size configurations are
+compared with the C restatement.  Bars (see golden_cases.tolerance): exact
+for median, morphology, integer box sums and integer-tap separable filters;
+within 1 LSB for integer outputs of FP32-accumulated sums, with the mismatch
+rate reported; float outputs within 1e-5 x max(1, |ref|).
+"""
+import numpy as np
+import pytest
+
+import golden_cases as G
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+CASES = G.case_ids()
+
+
+@pytest.mark.parametrize("idx", range(len(CASES)), ids=CASES)
+def test_golden_host_arrays(gpu, idx):
+    op, p, x, want = G.case(idx)
+    got = G.run_gpu(gpu, op, p, x)
+    G.compare(got, want, G.tolerance(op, p, x, want))
+
+
+@pytest.mark.parametrize("idx", range(0, len(CASES), 5), ids=CASES[::5])
+def test_golden_device_tensors(gpu, idx):
+    op, p, x, want = G.case(idx)
+    got = G.run_gpu(gpu, op, p, x, device_images=True)
+    G.compare(got, want, G.tolerance(op, p, x, want))
+
+
+def test_probe_border_index(gpu, orc):
+    import torch
+
+    from imageprocessingflex_b200 import _lib
+
+    lib = _lib.load()
+    p = torch.arange(-70, 71, dtype=torch.int32, device="cuda")
+    out = torch.empty_like(p)
+    for n in (1, 2, 3, 5, 8, 13):
+        for mode in oracle.BORDERS:
+            assert lib.ipfc_probe_border_index(p.data_ptr(), out.data_ptr(), p.numel(), n, mode, None) == 0
+            torch.cuda.synchronize()
+            want = [oracle.restatement().lib.orc_border_index(int(v), n, mode) for v in range(-70, 71)]
+            assert out.cpu().tolist() == want, (n, mode)
+
+
+def test_probe_saturate(gpu):
+    import ctypes
+
+    import torch
+
+    from imageprocessingflex_b200 import _lib
+
+    lib = _lib.load()
+    orc = oracle.restatement().lib
+    orc.orc_saturate.restype = ctypes.c_double
+    orc.orc_saturate.argtypes = [ctypes.c_double, ctypes.c_int]
+    vals = np.array([0.0, 0.5, -0.5, 0.49999997, 1.5, 2.5, -1.5, -2.5, 254.5, 255.49, 255.5, 256.0, -0.49999997,
+                     32766.5, 32767.5, -32768.5, -32769.0, 65534.5, 65535.5, 1e9, -1e9, np.inf, -np.inf, np.nan,
+                     0.49999997, 100.50001, 7.4999995], np.float32)
+    v = torch.from_numpy(vals).cuda()
+    for code, tdt in ((0, torch.uint8), (1, torch.uint16), (2, torch.int16), (4, torch.float32)):
+        out = torch.empty(vals.size, dtype=tdt, device="cuda")
+        assert lib.ipfc_probe_saturate(v.data_ptr(), out.data_ptr(), vals.size, code, None) == 0
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().astype(np.float64)
+        want = np.array([orc.orc_saturate(float(x), code) for x in vals])
+        np.testing.assert_array_equal(got, want, err_msg=f"dtype code {code}")
+
+
+# ---- known answers of the reference's unit tests, on the GPU ----------------
+
+def test_kat_impulse_and_constant(gpu):
+    B = gpu.BorderMode
+    impulse = np.zeros((7, 7), np.float32)
+    impulse[3, 3] = 1
+    r = gpu.filter2D(impulse, np.arange(1, 10, dtype=np.float32).reshape(3, 3), B.Constant)
+    assert r[2, 2] == 9 and r[4, 4] == 1 and r[2, 3] == 8
+    sep = gpu.sepFilter2D(impulse, [1, 2, 3], [4, 5, 6], B.Constant)
+    assert sep[2, 2] == 18 and sep[2, 4] == 6 and sep[4, 2] == 12
+    c = np.full((15, 20, 3), 77, np.uint8)
+    np.testing.assert_array_equal(gpu.gaussianBlur(c, 2.0), c)
+    np.testing.assert_array_equal(gpu.blur(c, 5), c)
+    np.testing.assert_array_equal(gpu.medianBlur(c, 5), c)
+    np.testing.assert_array_equal(gpu.medianBlur(c, 9), c)
+    for m in (B.Replicate, B.Reflect, B.Reflect101, B.Wrap):
+        np.testing.assert_array_equal(gpu.boxFilter(c, 4, 6, True, m), c)
+
+
+def test_kat_gradients(gpu):
+    y, x = np.mgrid[0:16, 0:16]
+    ramp = (3 * x + 2 * y).astype(np.float32)
+    assert abs(gpu.sobel(ramp, 1, 0)[8, 8] - 24) < 1e-4
+    assert abs(gpu.sobel(ramp, 0, 1)[8, 8] - 16) < 1e-4
+    assert abs(gpu.sobel(ramp, 1, 0, 1)[8, 8] - 6) < 1e-4
+    assert abs(gpu.sobel(ramp, 1, 0, 5)[8, 8] - 384) < 1e-3
+
+
+def test_kat_morphology(gpu):
+    img = np.zeros((9, 9), np.uint8)
+    img[3:6, 3:6] = 255
+    er = gpu.erode(img)
+    assert np.count_nonzero(er) == 1 and er[4, 4] == 255
+    di = gpu.dilate(img)
+    assert np.count_nonzero(di) == 25
+    np.testing.assert_array_equal(gpu.erode(di), img)
+    cross = gpu.dilate(er, gpu.getStructuringElement(gpu.MorphShape.Cross, 3))
+    assert np.count_nonzero(cross) == 5
+    np.testing.assert_array_equal(gpu.dilate(er, None, 2), gpu.dilate(er, gpu.getStructuringElement(0, 5)))
+    white = np.full((4, 6, 2), 255, np.uint8)
+    np.testing.assert_array_equal(gpu.erode(white, gpu.getStructuringElement(gpu.MorphShape.Ellipse, 5)), white)
+
+
+# ---- seeded random cases and edge shapes vs the restatement -----------------
+
+EDGE_SHAPES = [(1, 1, 1), (1, 7, 3), (9, 1, 1), (2, 3, 4), (3, 2, 2), (17, 5, 3), (130, 33, 1), (257, 70, 3),
+               (64, 64, 4)]
+
+
+@pytest.mark.parametrize("shape", EDGE_SHAPES, ids=lambda s: "x".join(map(str, s)))
+def test_random_cases_vs_restatement(gpu, orc, shape):
+    w, h, c = shape
+    rng = np.random.default_rng(w * 1000 + h * 10 + c)
+    B = gpu.BorderMode
+    for dt in (np.uint8, np.float32, np.uint16, np.int16):
+        img = oracle.random_image(w, h, c, dt, w + 3 * h + c)
+        for b in oracle.BORDERS:
+            for kw, kh in ((3, 3), (13, 13), (4, 2), (1, 5), (31, 7)):
+                kx, ky = rng.normal(size=kw), rng.normal(size=kh)
+                for od in (None, np.float32, np.int16):
+                    got = gpu.sepFilter2D(img, kx, ky, B(b), 0.3, 2.0, dtype=od)
+                    want = orc.sep_filter(img, kx, ky, border=b, delta=0.3, border_value=2.0, out_dtype=od)
+                    x = {"src": img, "kx": kx, "ky": ky}
+                    G.compare(got, want, G.tolerance("sep", {}, x, want))
+                k2 = rng.normal(size=(kh, kw)).astype(np.float32)
+                got = gpu.filter2D(img, k2, B(b), 0.5, (-1, -1), 7.0)
+                want = orc.filter2d(img, k2, b, 0.5, (-1, -1), 7.0)
+                G.compare(got, want, G.tolerance("filter2d", {}, {"src": img}, want))
+                for norm in (True, False):
+                    for od in (None, np.float32):
+                        got = gpu.boxFilter(img, kw, kh, norm, B(b), 3.0, dtype=od)
+                        want = orc.box_filter(img, kw, kh, norm, b, 3.0, od)
+                        G.compare(got, want, G.tolerance("box", {}, {"src": img}, want))
+            if b != 0:
+                for k in (1, 3, 5, 7, 9):
+                    np.testing.assert_array_equal(gpu.medianBlur(img, k, B(b)), orc.median_blur(img, k, b))
+        for shp in (0, 1, 2):
+            for sw, sh in ((3, 3), (5, 7), (4, 2), (1, 1)):
+                se = orc.structuring_element(shp, sw, sh)
+                for it in (0, 1, 3):
+                    np.testing.assert_array_equal(gpu.erode(img, se, it), orc.erode(img, se, it))
+                    np.testing.assert_array_equal(gpu.dilate(img, se, it), orc.dilate(img, se, it))
+
+
+def test_box_exact_ties_u8(gpu, orc):
+    """Even windows give exact x.5 means; the rounding must follow the
+    reference's FP64 expression tie by tie."""
+    rng = np.random.default_rng(5)
+    img = rng.integers(0, 256, size=(64, 96, 1), dtype=np.uint8)
+    for kw, kh in ((2, 1), (2, 2), (4, 4), (6, 2), (8, 8), (10, 6), (2, 50)):
+        for b in oracle.BORDERS:
+            np.testing.assert_array_equal(gpu.boxFilter(img, kw, kh, True, gpu.BorderMode(b), 3.0),
+                                          orc.box_filter(img, kw, kh, True, b, 3.0))
+
+
+def test_long_taps_two_pass_form(gpu, orc):
+    """Kernels longer than the fused form takes (two-pass with scratch)."""
+    img = oracle.random_image(300, 120, 2, np.float32, 4)
+    rng = np.random.default_rng(9)
+    kx, ky = rng.normal(size=101), rng.normal(size=67)
+    kx /= kx.sum()
+    ky /= ky.sum()
+    for b in oracle.BORDERS:
+        got = gpu.sepFilter2D(img, kx, ky, gpu.BorderMode(b), 0.1, 0.5)
+        want = orc.sep_filter(img, kx, ky, border=b, delta=0.1, border_value=0.5)
+        G.compare(got, want, ("rel", 1e-5))
+
+
+# ---- full-size configurations ------------------------------------------------
+
+def _lsb_report(got, want, label):
+    d = np.abs(got.astype(np.int32) - want.astype(np.int32))
+    assert d.max() <= 1, f"{label}: max |diff| {d.max()}"
+    rate = float((d > 0).mean())
+    print(f"\n{label}: mismatch rate {rate:.3e} ({int((d > 0).sum())} of {d.size} samples), max 1 LSB")
+    return rate
+
+
+def test_fullsize_gaussian_u8_rgb(gpu, orc):
+    """gaussianBlur sigma=2 (13 taps), 1920x1080x3 and 3840x2160x3 uint8, Reflect101."""
+    for w, h in ((1920, 1080), (3840, 2160)):
+        img = oracle.random_image(w, h, 3, np.uint8, 1)
+        got = gpu.gaussianBlur(img, 2.0)
+        want = orc.gaussian_blur(img, 2.0)
+        rate = _lsb_report(got, want, f"gaussian {w}x{h}x3")
+        assert rate < 1e-4
+
+
+def test_fullsize_sobel_int16_exact(gpu, orc):
+    img = oracle.random_image(3840, 2160, 1, np.uint8, 2)
+    for ksize in (3, 5):
+        for dx, dy in ((1, 0), (0, 1)):
+            got = gpu.sobel(img, dx, dy, ksize, dtype=np.int16)
+            kx, ky = orc.sobel_taps(dx, dy, ksize)
+            want = orc.sep_filter(img, kx, ky, out_dtype=np.int16)
+            np.testing.assert_array_equal(got, want)
+
+
+def test_fullsize_sep_f32(gpu, orc):
+    img = oracle.random_image(3840, 2160, 1, np.float32, 3)
+    rng = np.random.default_rng(11)
+    for L in (3, 31):
+        kx, ky = rng.normal(size=L), rng.normal(size=L)
+        kx /= kx.sum()
+        ky /= ky.sum()
+        for b in (0, 3):
+            got = gpu.sepFilter2D(img, kx, ky, gpu.BorderMode(b))
+            want = orc.sep_filter(img, kx, ky, border=b)
+            d = np.abs(got.astype(np.float64) - want)
+            assert d.max() <= 1e-5, d.max()
