@@ -35,6 +35,7 @@ DBL_P = ctypes.POINTER(c_double)
 _SIGNATURES = {
     "ipfc_last_error": (ctypes.c_char_p, []),
     "ipfc_version": (c_int, []),
+    "ipfc_check_device": (c_int, [c_void_p]),
     "ipfc_gaussian_kernel_1d": (c_int, [c_double, c_int, c_void_p, c_int]),
     "ipfc_deriv_kernel": (c_int, [c_int, c_int, c_void_p, c_int]),
     "ipfc_structuring_element": (c_int, [c_int, c_int, c_int, c_void_p]),

@@ -9,12 +9,15 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/ipfc.h"
 #include "kernels.cuh"
+#include "sep_fast_launch.cuh"
+#include "tma.cuh"
 
 namespace ipfc {
 
@@ -88,6 +91,46 @@ cudaError_t prepare_device() {
     return cudaSuccess;
 }
 
+// Device error word: kernels with bounded waits record a code here when a
+// wait gives up.  One word per device, allocated on the first call that
+// launches such a kernel on that device.
+static unsigned* g_err_word[32] = {nullptr};
+
+unsigned* device_error_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    unsigned*& w = g_err_word[dev & 31];
+    if (!w) {
+        unsigned* p = nullptr;
+        if (cudaMalloc((void**)&p, sizeof(unsigned)) != cudaSuccess ||
+            cudaMemset(p, 0, sizeof(unsigned)) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        w = p;
+    }
+    return w;
+}
+
+// Reads and clears the error word after the stream has drained.
+static int take_device_error(cudaStream_t s, const char* fn) {
+    unsigned* w = device_error_word();
+    if (!w) return IPFC_OK;
+    unsigned v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, w, sizeof(v), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    if (v == 0) return IPFC_OK;
+    cudaMemsetAsync(w, 0, sizeof(unsigned), s);
+    cudaStreamSynchronize(s);
+    return set_error(IPFC_ERR_TIMEOUT,
+                     "ipf: %s: a device-side wait gave up (code 0x%x); results of the affected call are not valid", fn,
+                     v);
+}
+
 // A device view of an image: the caller's memory, or a staged copy.
 struct DevView {
     void* ptr = nullptr;
@@ -137,7 +180,10 @@ static int finish(const ipfc_image* dst, DevView* in, DevView* out, cudaStream_t
     if (in && in->owned) cudaFreeAsync(in->ptr, s);
     if (out->owned) cudaFreeAsync(out->ptr, s);
     if (e != cudaSuccess) return cuda_status(e, fn);
-    if ((in && in->owned) || out->owned) IPFC_TRY_CUDA(cudaStreamSynchronize(s), fn);
+    if ((in && in->owned) || out->owned) {
+        IPFC_TRY_CUDA(cudaStreamSynchronize(s), fn);
+        return take_device_error(s, fn);
+    }
     return IPFC_OK;
 }
 
@@ -225,6 +271,97 @@ int deriv_taps(int order, int ksize, std::vector<double>& k) {
 // ---------------------------------------------------------------------------
 // Separable path shared by sepFilter2D, gaussianBlur and sobel.
 // ---------------------------------------------------------------------------
+
+// Kernel selection for separable filters: IPFC_SEP_PATH=generic forces the
+// generic fused/two-pass kernels (used to check one form against the other).
+static int sep_path_mode() {
+    static int mode = -1;
+    if (mode < 0) {
+        const char* v = std::getenv("IPFC_SEP_PATH");
+        mode = (v && std::strcmp(v, "generic") == 0) ? 1 : 0;
+    }
+    return mode;
+}
+
+// The fast kernel covers equal tap counts up to kFastMaxTaps with centred
+// anchors and finite taps; the instantiation table decides the rest.
+static bool sep_fast_eligible(const ipfc_image* src, const double* kx, int kw, const double* ky, int kh, int ax,
+                              int ay) {
+    if (sep_path_mode() == 1) return false;
+    if (kw != kh || kw > kFastMaxTaps || ax != kw / 2 || ay != kh / 2) return false;
+    if (src->channels != 1 && src->channels != 3 && src->channels != 4) return false;
+    for (int i = 0; i < kw; ++i)
+        if (!std::isfinite(kx[i]) || !std::isfinite(ky[i]) || !std::isfinite((float)kx[i]) ||
+            !std::isfinite((float)ky[i]))
+            return false;
+    return true;
+}
+
+static unsigned long long pack_tap2(double v) {
+    const float fv = (float)v;
+    unsigned u;
+    std::memcpy(&u, &fv, sizeof(u));
+    return ((unsigned long long)u << 32) | u;
+}
+
+// Launches the fast kernel when a fitting instantiation exists; returns
+// whether it did (e holds the launch status).
+static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const DevView& in, const DevView& out,
+                         const double* kx, int kw, const double* ky, int kh, int ax, int ay, int border, double delta,
+                         double bv, cudaStream_t s, cudaError_t* e) {
+    if (!sep_fast_eligible(src, kx, kw, ky, kh, ax, ay)) return false;
+    SepFastArgs f;
+    std::memset(&f, 0, sizeof(f));
+    f.src = in.ptr;
+    f.spitch = in.pitch;
+    f.dst = out.ptr;
+    f.dpitch = out.pitch;
+    f.W = src->width;
+    f.H = src->height;
+    f.border = border;
+    f.delta = (float)delta;
+    f.bv = (float)bv;
+    for (int i = 0; i < kw; ++i) {
+        f.kx[i] = (float)kx[i];
+        f.kx2[i] = pack_tap2(kx[i]);
+    }
+    for (int j = 0; j < kh; ++j) f.ky2[j] = pack_tap2(ky[j]);
+    const uintptr_t op = (uintptr_t)out.ptr, ip = (uintptr_t)in.ptr;
+    f.vec_store = (op % 16 == 0 && out.pitch % 16 == 0) ? 1 : 0;
+    const unsigned vec_align = src->dtype == IPFC_F32 ? 8u : 4u;  // 2 floats or 4 bytes per load
+    f.vec_load = (ip % vec_align == 0 && in.pitch % vec_align == 0) ? 1 : 0;
+    // Saturation is needed unless every output provably stays inside the
+    // destination range: non-negative taps bound the result between
+    // delta + sum(kx)sum(ky) * min(0, lowest input) and the same with the
+    // highest input.
+    f.clamp = 1;
+    if (dst->dtype == IPFC_U8 || dst->dtype == IPFC_U16) {
+        double sx = 0, sy = 0;
+        bool nonneg = true;
+        for (int i = 0; i < kw; ++i) {
+            sx += kx[i];
+            nonneg = nonneg && kx[i] >= 0;
+        }
+        for (int j = 0; j < kh; ++j) {
+            sy += ky[j];
+            nonneg = nonneg && ky[j] >= 0;
+        }
+        const double smax = src->dtype == IPFC_U8 ? 255.0 : 65535.0;
+        const double hi_in = border == IPFC_BORDER_CONSTANT ? std::fmax(smax, bv) : smax;
+        const double lo_in = border == IPFC_BORDER_CONSTANT ? std::fmin(0.0, bv) : 0.0;
+        const double dmax = dst->dtype == IPFC_U8 ? 255.0 : 65535.0;
+        if (nonneg && (src->dtype == IPFC_U8 || src->dtype == IPFC_U16) && delta + sx * sy * lo_in > -0.25 &&
+            delta + sx * sy * hi_in < dmax + 0.25)
+            f.clamp = 0;
+    }
+    f.err = device_error_word();
+    if (src->dtype == IPFC_U8)
+        f.use_tma =
+            encode_row_map_u32(&f.tmap, in.ptr, (long long)src->width * src->channels, src->height, in.pitch, kRingWords)
+                ? 1
+                : 0;
+    return sep_fast_dispatch(kw, src->channels, src->dtype, dst->dtype, f, s, e);
+}
 static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh, int ax,
                    int ay, int border, double delta, double bv, cudaStream_t s, const char* fn) {
     if (!kx || !ky || kw <= 0 || kh <= 0)
@@ -264,6 +401,11 @@ static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int
     float* dtaps = nullptr;
     float* scratch = nullptr;
     cudaError_t e = cudaSuccess;
+    if (run_sep_fast(src, dst, in, out, kx, kw, ky, kh, ax, ay, border, delta, bv, s, &e)) {
+        rc = finish(dst, &in, &out, s, fn);
+        if (e != cudaSuccess) return cuda_status(e, fn);
+        return rc;
+    }
     if (sep_needs_scratch(a)) {
         std::vector<float> taps((size_t)kw + kh);
         for (int i = 0; i < kw; ++i) taps[i] = (float)kx[i];
@@ -291,6 +433,17 @@ extern "C" {
 const char* ipfc_last_error(void) { return g_last_error.c_str(); }
 
 int ipfc_version(void) { return (1 << 16) | (0 << 8) | 0; }
+
+int ipfc_check_device(void* stream) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return set_error(IPFC_ERR_CUDA, "ipf: check_device: no CUDA device available");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    IPFC_TRY_CUDA(cudaStreamSynchronize(s), "check_device");
+    return take_device_error(s, "check_device");
+}
 
 int ipfc_gaussian_kernel_1d(double sigma, int ksize, double* out, int cap) {
     std::vector<double> k;

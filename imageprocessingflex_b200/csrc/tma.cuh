@@ -1,0 +1,96 @@
+// tma.cuh -- mbarrier and TMA (cp.async.bulk.tensor) helpers, sm_100a.
+//
+// Every wait is bounded: try_wait spins at most kSpinLimit times; on expiry
+// the caller's error word gets the given code (first writer wins) and the
+// wait returns false, so a kernel never spins forever and the host can
+// report IPFC_ERR_TIMEOUT.  No multicast form is used anywhere.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ipfc {
+
+// About 2^24 polls (tens of milliseconds): far above any legitimate wait
+// for a TMA row load, short enough to bound a stuck kernel.
+constexpr unsigned kSpinLimit = 1u << 24;
+
+// Error codes written to the device error word.
+constexpr unsigned kErrWaitFull = 0x101u;   // a TMA row never arrived
+constexpr unsigned kErrWaitEmpty = 0x102u;  // consumers never released a stage
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Makes barrier initialisation visible to the async (TMA) proxy.
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase of the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned* err, unsigned code) {
+    for (unsigned i = 0; i < kSpinLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicCAS(err, 0u, code);
+    return false;
+}
+
+// 2-D tiled TMA load of the map's box at element coordinates {x, y} into
+// shared memory, completing its bytes on the mbarrier.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// L2 prefetch of the same box (no shared-memory destination).
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y)
+                 : "memory");
+}
+
+// Host: encodes a 2-D tensor map over rows of 32-bit words (row_bytes / 4
+// words, `rows` rows, `pitch` bytes apart) with a box of {box_words, 1}.
+// Returns false when the layout does not meet TMA's rules (16-byte aligned
+// base and pitch, whole words per row) or the driver call fails.
+bool encode_row_map_u32(CUtensorMap* map, const void* base, long long row_bytes, int rows, long long pitch,
+                        int box_words);
+
+}  // namespace ipfc

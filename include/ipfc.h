@@ -98,6 +98,12 @@ IPFC_API const char* ipfc_last_error(void);
 /* (major << 16) | (minor << 8) | patch of this library. */
 IPFC_API int ipfc_version(void);
 
+/* Waits for `stream`, then reports whether any kernel since the last check
+ * gave up a bounded device-side wait (IPFC_ERR_TIMEOUT; the word is then
+ * cleared).  Calls with host images check this themselves.  No counterpart
+ * in the reference, whose CPU code has no device waits. */
+IPFC_API int ipfc_check_device(void* stream);
+
 /* ---- tap and element generators (host, FP64) ----------------------------- */
 
 /* gaussianKernel1D (filter.hpp:129-145).  Writes min(len, cap) taps to out and
