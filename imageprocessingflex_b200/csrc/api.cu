@@ -354,12 +354,6 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
             delta + sx * sy * hi_in < dmax + 0.25)
             f.clamp = 0;
     }
-    f.err = device_error_word();
-    if (src->dtype == IPFC_U8)
-        f.use_tma =
-            encode_row_map_u32(&f.tmap, in.ptr, (long long)src->width * src->channels, src->height, in.pitch, kRingWords)
-                ? 1
-                : 0;
     return sep_fast_dispatch(kw, src->channels, src->dtype, dst->dtype, f, s, e);
 }
 static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh, int ax,

@@ -12,39 +12,30 @@
 //    source samples of the halo'd strip (4 for 8-bit sources, 2 for float),
 //    converts them once per row and scatters them into a ring of K
 //    accumulator pairs in registers with fma.rn.f32x2 (one instruction per
-//    two samples; every ring index is a compile-time constant).  For 8-bit
-//    sources on interior strips the rows arrive by TMA
-//    (cp.async.bulk.tensor, one strip row per box) in a ring of kRingStages
-//    shared-memory stages with full/empty mbarriers, refilled by thread 0 as
-//    the warps release stages, with L2 prefetches further ahead.  Edge
-//    strips resolve their border columns per thread and load K rows ahead
-//    through the read-only path.  Border rows take a non-inlined slow path.
+//    two samples; every ring index is a compile-time constant).  Each row's
+//    samples are loaded K rows ahead of use through the read-only path (one
+//    32-bit load per thread for 8-bit sources), border columns resolved per
+//    thread, border rows through a non-inlined slow path.
 //  * Finished column-pass rows go to shared memory split by channel
-//    (planar) with pairs of rows interleaved (row r and r+1 of a pixel are
-//    adjacent floats), TB = 2K rows per band.  Then the CTA switches to the
-//    row pass: one thread per (row pair, run of RUN output pixels) reads its
-//    window with 128-bit shared loads per channel, each of which yields
-//    aligned (row r, row r+1) operand pairs for fma.rn.f32x2, rounds with
-//    two packed round-toward-minus-infinity adds, byte-packs the interleaved
-//    output in registers with PRMT and stores it with 64/128-bit stores.
+//    (planar), TB = K rows per band.  Then the CTA switches to the row
+//    pass: one thread per (band row, run of RUN output pixels) reads its
+//    window with 128-bit shared loads per channel, accumulates the K
+//    horizontal taps, rounds pairs of outputs with two packed
+//    round-toward-minus-infinity adds, byte-packs the interleaved output in
+//    registers with PRMT and stores it with 64/128-bit stores.
 //
 // FP32 throughput bounds this kernel (2K multiply-adds per output sample);
 // the design keeps every other instruction per sample to a few.
 #pragma once
 
 #include "common.cuh"
-#include "tma.cuh"
 
 namespace ipfc {
 
 constexpr int kFastThreads = 256;
 constexpr int kFastMaxTaps = 32;
-constexpr int kRingStages = 6;      // TMA row stages per CTA (8-bit sources)
-constexpr int kRingWords = 256;     // one strip row: 1024 bytes
-constexpr int kPrefetchAhead = 12;  // rows prefetched into L2 beyond the ring
 
 struct SepFastArgs {
-    CUtensorMap tmap;  // 8-bit sources: rows as 32-bit words, box {kRingWords, 1}
     const void* src;
     long long spitch;
     void* dst;
@@ -58,8 +49,6 @@ struct SepFastArgs {
     int vec_store;  // destination base and pitch allow 8/16-byte stores
     int vec_load;   // source base and pitch allow NCOL-sample loads
     int clamp;      // outputs may leave the destination range: saturate
-    int use_tma;    // tmap is valid (16-byte aligned base and pitch, whole words per row)
-    unsigned* err;  // device error word (bounded waits that gave up), or null
     float kx[kFastMaxTaps];
     unsigned long long kx2[kFastMaxTaps];  // horizontal taps, each packed twice (f32x2)
     unsigned long long ky2[kFastMaxTaps];  // vertical taps, each packed twice (f32x2)
@@ -71,16 +60,16 @@ struct FastGeom {
     static constexpr int RUN = 8;            // output pixels per row-pass item
     static constexpr int RX = K / 2;         // left halo (pixels)
     static constexpr int HX = K - 1;         // total horizontal halo
-    // samples the threads cover; 8-bit strips start 16-byte aligned (TMA)
-    static constexpr int ALIGN = NCOL == 4 ? 16 : NCOL;
+    // samples the threads cover; thread groups start NCOL-aligned
+    static constexpr int ALIGN = NCOL;
     static constexpr int SPAN = NCOL * kFastThreads - (ALIGN - 1);
-    static constexpr int TB = 2 * K;         // band rows: an even multiple of K
+    static constexpr int TB = K;             // band rows: a multiple of K
     // utilisation (x1e6) of the column pass (threads with columns) times the
     // row pass (row-pair items over whole rounds) for strip width px
     static constexpr long long score(int px) {
         const int iw = (px + HX) * C;
         const int vthreads = (iw + NCOL - 1) / NCOL + 1;
-        const int items = K * (px / RUN);
+        const int items = TB * (px / RUN);
         const int rounds = (items + kFastThreads - 1) / kFastThreads;
         return (long long)1000000 * vthreads / kFastThreads * items / (rounds * kFastThreads);
     }
@@ -98,16 +87,13 @@ struct FastGeom {
     static constexpr int IW = (PX + HX) * C;  // source samples per strip row
     static constexpr int RUNS = PX / RUN;
     static constexpr int VW = PX + HX;        // plane row width (pixels)
-    // a row pair occupies 2*VWP floats; 2*VWP = 4 (mod 32) so lanes reading
-    // 16 B at the same column of consecutive row pairs hit distinct 16-byte
-    // bank groups
-    static constexpr int VWP = VW + ((2 - VW % 16) + 16) % 16;
-    static constexpr int PAIR = 2 * VWP;
-    static constexpr int PLANE = (TB / 2) * PAIR;
+    // row stride = 4 (mod 32) floats: lanes reading 16 B at the same column
+    // of consecutive rows hit distinct 16-byte bank groups
+    static constexpr int VW4 = (VW + 3) / 4 * 4;
+    static constexpr int VWP = VW4 + ((4 - VW4 % 32) + 32) % 32;
+    static constexpr int PLANE = TB * VWP;
     static constexpr size_t PLANES_BYTES = sizeof(float) * (size_t)C * PLANE;
-    static constexpr size_t RING_OFF = (PLANES_BYTES + 127) / 128 * 128;
-    static constexpr size_t BAR_OFF = RING_OFF + (NCOL == 4 ? (size_t)kRingStages * kRingWords * 4 : 0);
-    static constexpr size_t SMEM = BAR_OFF + (NCOL == 4 ? 2 * kRingStages * sizeof(uint64_t) : 0);
+    static constexpr size_t SMEM = PLANES_BYTES;
 };
 
 // ---- packed FP32 (fma/add .f32x2, sm_100a) ----------------------------------
@@ -184,6 +170,98 @@ __host__ __device__ constexpr unsigned byte_insert_sel(int pos) {
     return (0x3210u & ~(0xFu << (4 * pos))) | (4u << (4 * pos));
 }
 
+// ---- the row pass ------------------------------------------------------------
+// Row pass over one band: thread = (band row, run of RUN output pixels).
+// Inlined at its hot call site (once per band inside the unrolled loop);
+// sep_row_pass_cold is the out-of-line copy for the last, partial band.
+template <int K, int C, typename Tout, typename G>
+__device__ __forceinline__ void sep_row_pass(const SepFastArgs& a, const float* vbuf, int rows_in_band, int band_start,
+                                          int x0) {
+    __syncthreads();
+    for (int it = threadIdx.x; it < G::TB * G::RUNS; it += kFastThreads) {
+        const int r = it % G::TB, g = it / G::TB;
+        if (r >= rows_in_band) continue;
+        const int y = band_start + r;
+        const int p0 = g * G::RUN;  // strip-relative output pixel
+        constexpr int NWORDS = (G::RUN * C * (int)sizeof(Tout) + 3) / 4;
+        unsigned words[NWORDS];
+#pragma unroll
+        for (int w = 0; w < NWORDS; ++w) words[w] = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            constexpr int NW4 = (G::RUN + G::HX + 3) / 4;
+            float win[NW4 * 4];
+            const float4* src4 = reinterpret_cast<const float4*>(vbuf + c * G::PLANE + r * G::VWP + p0);
+#pragma unroll
+            for (int q = 0; q < NW4; ++q) {
+                const float4 v4 = src4[q];
+                win[4 * q] = v4.x;
+                win[4 * q + 1] = v4.y;
+                win[4 * q + 2] = v4.z;
+                win[4 * q + 3] = v4.w;
+            }
+#pragma unroll
+            for (int u = 0; u < G::RUN; u += 2) {
+                float2 s = make_float2(a.delta, a.delta);
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    s.x = fmaf(a.kx[i], win[u + i], s.x);
+                    s.y = fmaf(a.kx[i], win[u + 1 + i], s.y);
+                }
+                const int e0 = u * C + c, e1 = (u + 1) * C + c;  // interleaved positions
+                if constexpr (sizeof(Tout) == 1) {
+                    if (a.clamp) s = make_float2(fminf(fmaxf(s.x, 0.f), 255.f), fminf(fmaxf(s.y, 0.f), 255.f));
+                    const float2 m = round_pair_u(s);
+                    // the byte is the low byte of the float's bit pattern
+                    words[e0 >> 2] = __byte_perm(words[e0 >> 2], __float_as_uint(m.x), byte_insert_sel(e0 & 3));
+                    words[e1 >> 2] = __byte_perm(words[e1 >> 2], __float_as_uint(m.y), byte_insert_sel(e1 & 3));
+                } else if constexpr (std::is_same<Tout, int16_t>::value) {
+                    words[e0 >> 1] |= (unsigned)(round_s_sat(s.x, -32768, 32767) & 0xffff) << (16 * (e0 & 1));
+                    words[e1 >> 1] |= (unsigned)(round_s_sat(s.y, -32768, 32767) & 0xffff) << (16 * (e1 & 1));
+                } else if constexpr (std::is_same<Tout, uint16_t>::value) {
+                    if (a.clamp)
+                        s = make_float2(fminf(fmaxf(s.x, 0.f), 65535.f), fminf(fmaxf(s.y, 0.f), 65535.f));
+                    const float2 m = round_pair_u(s);
+                    words[e0 >> 1] |= (__float_as_uint(m.x) & 0xffffu) << (16 * (e0 & 1));
+                    words[e1 >> 1] |= (__float_as_uint(m.y) & 0xffffu) << (16 * (e1 & 1));
+                } else {
+                    words[e0] = __float_as_uint(s.x);
+                    words[e1] = __float_as_uint(s.y);
+                }
+            }
+        }
+        if (y >= a.H) continue;
+        const int px = x0 + p0;
+        constexpr int NBYTES = G::RUN * C * (int)sizeof(Tout);
+        unsigned char* db =
+            reinterpret_cast<unsigned char*>(row_ptr_mut<Tout>(a.dst, a.dpitch, y)) + (size_t)px * C * sizeof(Tout);
+        if (px + G::RUN <= a.W && a.vec_store) {
+            if constexpr (NBYTES % 16 == 0) {
+#pragma unroll
+                for (int q = 0; q < NBYTES / 16; ++q)
+                    reinterpret_cast<uint4*>(db)[q] =
+                        make_uint4(words[4 * q], words[4 * q + 1], words[4 * q + 2], words[4 * q + 3]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < NBYTES / 8; ++q)
+                    reinterpret_cast<uint2*>(db)[q] = make_uint2(words[2 * q], words[2 * q + 1]);
+            }
+        } else {
+            const int nbytes = min(G::RUN, a.W - px) * C * (int)sizeof(Tout);
+#pragma unroll
+            for (int e = 0; e < NBYTES; ++e)
+                if (e < nbytes) db[e] = (unsigned char)((words[e >> 2] >> (8 * (e & 3))) & 0xffu);
+        }
+    }
+    __syncthreads();
+}
+
+template <int K, int C, typename Tout, typename G>
+__device__ __noinline__ void sep_row_pass_cold(const SepFastArgs& a, const float* vbuf, int rows_in_band,
+                                               int band_start, int x0) {
+    sep_row_pass<K, C, Tout, G>(a, vbuf, rows_in_band, band_start, x0);
+}
+
 // ---- the kernel -------------------------------------------------------------
 template <int K, int C, typename Tin, typename Tout>
 __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
@@ -191,8 +269,7 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
     constexpr int NCOL = sizeof(Tin) == 1 ? 4 : 2;
     constexpr int NP = NCOL / 2;  // accumulator pairs per ring slot
     using G = FastGeom<K, C, NCOL>;
-    extern __shared__ __align__(128) float vbuf[];  // C planes x TB/2 row pairs x PAIR
-    __shared__ volatile int s_abort;
+    extern __shared__ __align__(128) float vbuf[];  // C planes x TB rows x VWP
     const int tid = threadIdx.x;
     const int strip = blockIdx.x % a.strips;
     const int chunk = blockIdx.x / a.strips;
@@ -204,7 +281,7 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
 
     // --- this thread's NCOL source columns: strip-relative samples s0 .. s0+NCOL-1
     const int g0 = (x0 - G::RX) * C;               // global sample of strip sample 0
-    const int lead = g0 & (G::ALIGN - 1);          // thread groups start on an ALIGN-aligned global sample
+    const int lead = g0 & (G::ALIGN - 1);          // thread groups start on an aligned global sample
     const int s0 = NCOL * tid - lead;
     const bool active = s0 + NCOL - 1 >= 0 && s0 < G::IW;
     int idx[NCOL];
@@ -223,7 +300,7 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
 #pragma unroll
     for (int k = 0; k < NCOL; ++k) {
         const int s = s0 + k;
-        vdst[k] = (active && s >= 0 && s < G::IW) ? (s % C) * G::PLANE + 2 * (s / C) : -1;
+        vdst[k] = (active && s >= 0 && s < G::IW) ? (s % C) * G::PLANE + s / C : -1;
     }
 
     f2p acc[K][NP];
@@ -237,145 +314,13 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
     int band_row = 0;                              // rows filled in the band buffer
     int band_start = r0;                           // image row of band row 0
 
-    // ---- TMA row ring (8-bit sources, strips whose columns are all inside)
-    unsigned char* ring = reinterpret_cast<unsigned char*>(vbuf) + G::RING_OFF;
-    uint64_t* full = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(vbuf) + G::BAR_OFF);
-    uint64_t* empty = full + kRingStages;
-    const bool use_tma = NCOL == 4 && a.use_tma && g0 >= 0 && g0 + G::IW <= rowlen;
-    const int xw = (g0 - lead) / 4;                // box origin in 32-bit words (16-byte aligned)
-    // A bounded wait that gives up sets the CTA-wide abort flag: every thread
-    // then stops waiting (each has at most one expired wait), the CTA still
-    // meets every barrier and finishes, and the host reads the error word.
-    int issued = 0;                                // thread 0: rows handed to TMA
-    int consumed = 0;                              // thread 0: rows read from the ring
-    auto wait_or_abort = [&](uint64_t* bar, unsigned par, unsigned code) {
-        if (s_abort) return;
-        if (!mbar_wait(bar, par, a.err, code)) s_abort = 1;
-    };
-    auto issue_row = [&](int t) {                  // thread 0: load source row t into its stage
-        const int st = t % kRingStages;
-        const int sy = row_source(ybase + t, a.H, a.border);
-        if (sy >= 0) {
-            mbar_arrive_expect_tx(&full[st], kRingWords * 4);
-            tma_load_2d(ring + st * kRingWords * 4, &a.tmap, xw, sy, &full[st]);
-        } else {
-            mbar_arrive(&full[st]);                // Constant row: nothing to load
-        }
-        issued = t + 1;
-        const int tp = t + kPrefetchAhead;
-        if (tp < T) {
-            const int py = row_source(ybase + tp, a.H, a.border);
-            if (py >= 0) tma_prefetch_2d(&a.tmap, xw, py);
-        }
-    };
-    if (tid == 0) s_abort = 0;
-    if constexpr (NCOL == 4) {
-        if (use_tma && tid == 0) {
-            for (int st = 0; st < kRingStages; ++st) {
-                mbar_init(&full[st], 1);
-                mbar_init(&empty[st], kFastThreads / 32);
-            }
-            fence_barrier_init();
-        }
-    }
-    __syncthreads();
-    if constexpr (NCOL == 4) {
-        if (use_tma && tid == 0)
-            for (int t = 0; t < kRingStages && t < T; ++t) issue_row(t);
-    }
-
-    // ------------------------------------------------------------------ row pass
-    auto row_pass = [&](int rows_in_band) {
-        __syncthreads();
-        constexpr int NPAIRS = G::TB / 2;
-        for (int it = tid; it < NPAIRS * G::RUNS; it += kFastThreads) {
-            const int pr = it % NPAIRS, g = it / NPAIRS;
-            if (2 * pr >= rows_in_band) continue;
-            const int p0 = g * G::RUN;             // strip-relative output pixel
-            constexpr int NWORDS = (G::RUN * C * (int)sizeof(Tout) + 3) / 4;
-            unsigned words[2][NWORDS];             // output rows 2pr and 2pr+1
-#pragma unroll
-            for (int w = 0; w < NWORDS; ++w) words[0][w] = words[1][w] = 0;
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-                // win[2k], win[2k+1]: pixel p0+k of rows 2pr, 2pr+1
-                constexpr int NW4 = (2 * (G::RUN + G::HX) + 3) / 4;
-                float win[NW4 * 4];
-                const float4* src4 = reinterpret_cast<const float4*>(vbuf + c * G::PLANE + pr * G::PAIR + 2 * p0);
-#pragma unroll
-                for (int q = 0; q < NW4; ++q) {
-                    const float4 v4 = src4[q];
-                    win[4 * q] = v4.x;
-                    win[4 * q + 1] = v4.y;
-                    win[4 * q + 2] = v4.z;
-                    win[4 * q + 3] = v4.w;
-                }
-                const f2p dd = pk2(a.delta, a.delta);
-#pragma unroll
-                for (int u = 0; u < G::RUN; ++u) {
-                    f2p sp = dd;
-#pragma unroll
-                    for (int i = 0; i < K; ++i) sp = ffma2p(a.kx2[i], pk2(win[2 * (u + i)], win[2 * (u + i) + 1]), sp);
-                    float2 s = upk2(sp);
-                    const int e = u * C + c;  // interleaved position within the run
-                    if constexpr (sizeof(Tout) == 1) {
-                        if (a.clamp)
-                            s = make_float2(fminf(fmaxf(s.x, 0.f), 255.f), fminf(fmaxf(s.y, 0.f), 255.f));
-                        const float2 m = round_pair_u(s);
-                        // the byte is the low byte of the float's bit pattern
-                        words[0][e >> 2] = __byte_perm(words[0][e >> 2], __float_as_uint(m.x), byte_insert_sel(e & 3));
-                        words[1][e >> 2] = __byte_perm(words[1][e >> 2], __float_as_uint(m.y), byte_insert_sel(e & 3));
-                    } else if constexpr (std::is_same<Tout, int16_t>::value) {
-                        words[0][e >> 1] |= (unsigned)(round_s_sat(s.x, -32768, 32767) & 0xffff) << (16 * (e & 1));
-                        words[1][e >> 1] |= (unsigned)(round_s_sat(s.y, -32768, 32767) & 0xffff) << (16 * (e & 1));
-                    } else if constexpr (std::is_same<Tout, uint16_t>::value) {
-                        if (a.clamp)
-                            s = make_float2(fminf(fmaxf(s.x, 0.f), 65535.f), fminf(fmaxf(s.y, 0.f), 65535.f));
-                        const float2 m = round_pair_u(s);
-                        words[0][e >> 1] |= (__float_as_uint(m.x) & 0xffffu) << (16 * (e & 1));
-                        words[1][e >> 1] |= (__float_as_uint(m.y) & 0xffffu) << (16 * (e & 1));
-                    } else {
-                        words[0][e] = __float_as_uint(s.x);
-                        words[1][e] = __float_as_uint(s.y);
-                    }
-                }
-            }
-            const int px = x0 + p0;
-            constexpr int NBYTES = G::RUN * C * (int)sizeof(Tout);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int y = band_start + 2 * pr + h;
-                if (2 * pr + h >= rows_in_band || y >= a.H) continue;
-                unsigned char* db = reinterpret_cast<unsigned char*>(row_ptr_mut<Tout>(a.dst, a.dpitch, y)) +
-                                    (size_t)px * C * sizeof(Tout);
-                if (px + G::RUN <= a.W && a.vec_store) {
-                    if constexpr (NBYTES % 16 == 0) {
-#pragma unroll
-                        for (int q = 0; q < NBYTES / 16; ++q)
-                            reinterpret_cast<uint4*>(db)[q] = make_uint4(words[h][4 * q], words[h][4 * q + 1],
-                                                                         words[h][4 * q + 2], words[h][4 * q + 3]);
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < NBYTES / 8; ++q)
-                            reinterpret_cast<uint2*>(db)[q] = make_uint2(words[h][2 * q], words[h][2 * q + 1]);
-                    }
-                } else {
-                    const int nbytes = min(G::RUN, a.W - px) * C * (int)sizeof(Tout);
-#pragma unroll
-                    for (int e = 0; e < NBYTES; ++e)
-                        if (e < nbytes) db[e] = (unsigned char)((words[h][e >> 2] >> (8 * (e & 3))) & 0xffu);
-                }
-            }
-        }
-        __syncthreads();
-    };
-
     // ------------------------------------------------------------- column pass
+    // The raw samples of the next K rows, loaded K rows ahead of use.
     using Raw = typename std::conditional<sizeof(Tin) == 1, unsigned, uint2>::type;
     Raw raw[K];
     auto fetch = [&](int t) -> Raw {
         Raw r{};
-        if (t < T && active && !use_tma) {
+        if (t < T && active) {
             const int sy = row_source(ybase + t, a.H, a.border);
             if (sy >= 0) {
                 const Tin* srow = row_ptr<Tin>(a.src, a.spitch, sy);
@@ -387,7 +332,7 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
                         for (int k = 0; k < NCOL; ++k)
                             if (idx[k] >= 0) r |= (unsigned)__ldg(srow + idx[k]) << (8 * k);
                     }
-                } else if constexpr (sizeof(Tin) == 4) {
+                } else {
                     if (vec) {
                         const float2 v = __ldg(reinterpret_cast<const float2*>(srow + idx[0]));
                         r = make_uint2(__float_as_uint(v.x), __float_as_uint(v.y));
@@ -395,43 +340,13 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
                         if (idx[0] >= 0) r.x = __float_as_uint(static_cast<float>(__ldg(srow + idx[0])));
                         if (idx[1] >= 0) r.y = __float_as_uint(static_cast<float>(__ldg(srow + idx[1])));
                     }
-                } else {
-                    if (idx[0] >= 0) r.x = __float_as_uint(static_cast<float>(srow[idx[0]]));
-                    if (idx[1] >= 0) r.y = __float_as_uint(static_cast<float>(srow[idx[1]]));
                 }
             }
         }
         return r;
     };
-    // decoded samples of one row into NP packed pairs; Constant rows and
-    // columns read bv
-    const f2p mbias = pk2(-8388608.0f, -8388608.0f);
-    auto decode = [&](int t, Raw r, f2p (&x)[NP]) {
-        const int y = ybase + t;
-        const bool const_row = a.border == IPFC_BORDER_CONSTANT && (unsigned)y >= (unsigned)a.H;
-        if constexpr (sizeof(Tin) == 1) {
-            // byte k -> 2^23 + byte (PRMT into the mantissa), then one packed add
-#pragma unroll
-            for (int q = 0; q < NP; ++q) {
-                const unsigned f0 = __byte_perm(r, 0x4B000000u, 0x7440 | (2 * q));
-                const unsigned f1 = __byte_perm(r, 0x4B000000u, 0x7440 | (2 * q + 1));
-                x[q] = fadd2p(((f2p)f1 << 32) | f0, mbias);
-            }
-        } else {
-            x[0] = ((f2p)r.y << 32) | r.x;
-        }
-        if (const_row || cmask) {
-#pragma unroll
-            for (int q = 0; q < NP; ++q) {
-                float2 v = upk2(x[q]);
-                if (const_row || ((cmask >> (2 * q)) & 1u)) v.x = a.bv;
-                if (const_row || ((cmask >> (2 * q + 1)) & 1u)) v.y = a.bv;
-                x[q] = pk2(v.x, v.y);
-            }
-        }
-    };
-
     static_for<0, K>([&](auto U) { raw[decltype(U)::value] = fetch(decltype(U)::value); });
+    const f2p mbias = pk2(-8388608.0f, -8388608.0f);
 
     for (int tb = 0; tb < T; tb += K) {
         static_for<0, K>([&](auto U) {
@@ -439,29 +354,27 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
             const int t = tb + u;
             if (t < T) {
                 f2p x[NP];
-                if constexpr (NCOL == 4) {
-                    if (use_tma) {
-                        const int st = t % kRingStages;
-                        const unsigned par = (unsigned)(t / kRingStages) & 1u;
-                        wait_or_abort(&full[st], par, kErrWaitFull);
-                        const unsigned rw = reinterpret_cast<const unsigned*>(ring + st * kRingWords * 4)[tid];
-                        __syncwarp();
-                        if ((tid & 31) == 0) mbar_arrive(&empty[st]);
-                        if (tid == 0) {
-                            consumed = t + 1;
-                            if (t + kRingStages < T) {
-                                wait_or_abort(&empty[st], par, kErrWaitEmpty);
-                                if (!s_abort) issue_row(t + kRingStages);
-                            }
-                        }
-                        decode(t, rw, x);
-                    } else {
-                        decode(t, raw[u], x);
-                        raw[u] = fetch(t + K);
+                if constexpr (sizeof(Tin) == 1) {
+                    // byte k -> 2^23 + byte (PRMT into the mantissa), then one packed add
+#pragma unroll
+                    for (int q = 0; q < NP; ++q) {
+                        const unsigned f0 = __byte_perm(raw[u], 0x4B000000u, 0x7440 | (2 * q));
+                        const unsigned f1 = __byte_perm(raw[u], 0x4B000000u, 0x7440 | (2 * q + 1));
+                        x[q] = fadd2p(((f2p)f1 << 32) | f0, mbias);
                     }
                 } else {
-                    decode(t, raw[u], x);
-                    raw[u] = fetch(t + K);
+                    x[0] = ((f2p)raw[u].y << 32) | raw[u].x;
+                }
+                raw[u] = fetch(t + K);
+                const bool const_row = a.border == IPFC_BORDER_CONSTANT && (unsigned)(ybase + t) >= (unsigned)a.H;
+                if (const_row || cmask) {
+#pragma unroll
+                    for (int q = 0; q < NP; ++q) {
+                        float2 v = upk2(x[q]);
+                        if (const_row || ((cmask >> (2 * q)) & 1u)) v.x = a.bv;
+                        if (const_row || ((cmask >> (2 * q + 1)) & 1u)) v.y = a.bv;
+                        x[q] = pk2(v.x, v.y);
+                    }
                 }
                 // source row t feeds output o = t - j with tap j (ring slot (u - j) mod K)
                 static_for<0, K>([&](auto J) {
@@ -472,7 +385,7 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
                 });
                 constexpr int done = (u + 1) % K;  // slot of output t - (K - 1)
                 if (t >= K - 1) {
-                    const int off = (band_row >> 1) * G::PAIR + (band_row & 1);
+                    const int off = band_row * G::VWP;
 #pragma unroll
                     for (int q = 0; q < NP; ++q) {
                         if (vdst[2 * q] >= 0) vbuf[vdst[2 * q] + off] = lo_f(acc[done][q]);
@@ -483,11 +396,10 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
 #pragma unroll
                 for (int q = 0; q < NP; ++q) acc[done][q] = 0ull;
                 // TB is a multiple of K and the first output leaves at t = K-1,
-                // so a band always fills at ring position u = K-2: the row
-                // pass is emitted once, in that copy only.
+                // so a band always fills at ring position u = K-2.
                 if constexpr (u == K - 2) {
                     if (band_row == G::TB) {
-                        row_pass(G::TB);
+                        sep_row_pass<K, C, Tout, G>(a, vbuf, G::TB, band_start, x0);
                         band_start += G::TB;
                         band_row = 0;
                     }
@@ -495,12 +407,7 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
             }
         });
     }
-    if (band_row > 0) row_pass(band_row);
-    // After an abort, rows already handed to TMA may still be landing in this
-    // CTA's shared memory: wait for them (bounded) before the CTA retires.
-    if (NCOL == 4 && use_tma && tid == 0)
-        for (int t = consumed; t < issued; ++t)
-            mbar_wait(&full[t % kRingStages], (unsigned)(t / kRingStages) & 1u, nullptr, 0);
+    if (band_row > 0) sep_row_pass_cold<K, C, Tout, G>(a, vbuf, band_row, band_start, x0);
 }
 
 }  // namespace ipfc
