@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--launches-only", type=int, default=0,
+                    help="run this many launches of the workload on one resident image and exit (for ncu captures)")
     return ap.parse_args()
 
 
@@ -343,8 +345,25 @@ def run_ours(args):
     return 0
 
 
+def launches_only(n):
+    """n plain launches of the workload on one resident image, no timing:
+    the program profiled by the ncu captures summarised under profiles/."""
+    import torch
+
+    import imageprocessingflex_b200 as ipf
+
+    x = torch.from_numpy(seeded_image(W_IMG, H_IMG, C_IMG)).cuda()
+    for _ in range(n):
+        y = ipf.gaussianBlur(x, SIGMA)
+    torch.cuda.synchronize()
+    print(f"{n} launches done, checksum {int(y.sum().item())}")
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.launches_only > 0:
+        return launches_only(args.launches_only)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

@@ -1,0 +1,166 @@
+// ipf_cuda.hpp -- ipf::cuda: the neighbourhood-filter functions of
+// ImageProcessingFlex with the reference's own signatures, computed on a B200.
+//
+//   #include <ipf/ipf.hpp>        // the reference library (Image<T>, BorderMode, ...)
+//   #include <ipf_cuda.hpp>       // this header; link libipfcuda.so
+//
+//   ipf::ImageU8 out = ipf::cuda::gaussianBlur(img, 2.0);   // was ipf::gaussianBlur
+//
+// Each function takes and returns ipf::Image<T> by value exactly like its
+// ipf:: counterpart (same template parameters, defaults and error type); the
+// call copies the image to the device, runs the CUDA kernel and copies the
+// result back through the C ABI of ipfc.h.  Argument errors throw
+// ipf::Error with the reference's "ipf: <function>: <reason>" text.  There
+// is no CPU fallback: without a usable GPU the calls throw.
+//
+// Element types provided: uint8, uint16, int16 and float (ImageU8, ImageU16,
+// ImageI16, ImageF); ImageI32 and ImageD throw ipf::Error.
+#pragma once
+
+#include <ipf/filter.hpp>
+#include <ipf/morphology.hpp>
+
+#include <cstdint>
+#include <type_traits>
+#include <vector>
+
+#include "ipfc.h"
+
+namespace ipf {
+namespace cuda {
+
+namespace detail {
+
+template <class TOut, class T>
+using OutT = std::conditional_t<std::is_void<TOut>::value, T, TOut>;
+
+template <class T>
+constexpr int dtype_of() {
+    if constexpr (std::is_same<T, std::uint8_t>::value) return IPFC_U8;
+    else if constexpr (std::is_same<T, std::uint16_t>::value) return IPFC_U16;
+    else if constexpr (std::is_same<T, std::int16_t>::value) return IPFC_I16;
+    else if constexpr (std::is_same<T, std::int32_t>::value) return IPFC_I32;
+    else if constexpr (std::is_same<T, float>::value) return IPFC_F32;
+    else return IPFC_F64;
+}
+
+template <class T>
+ipfc_image view(const Image<T>& im) {
+    ipfc_image v;
+    v.data = const_cast<T*>(im.data());
+    v.width = im.width();
+    v.height = im.height();
+    v.channels = im.channels();
+    v.dtype = dtype_of<T>();
+    v.pitch = 0;
+    v.mem = IPFC_MEM_HOST;
+    return v;
+}
+
+inline void check(int rc) {
+    if (rc != IPFC_OK) throw ipf::Error(ipfc_last_error());
+}
+
+}  // namespace detail
+
+/// sepFilter2D (include/ipf/filter.hpp:197-203).
+template <class TOut = void, class T>
+Image<detail::OutT<TOut, T>> sepFilter2D(const Image<T>& src, const std::vector<double>& kx,
+                                         const std::vector<double>& ky, BorderMode border = BorderMode::Reflect101,
+                                         double delta = 0.0, double borderValue = 0.0) {
+    Image<detail::OutT<TOut, T>> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_sep_filter2d(&s, &d, kx.data(), static_cast<int>(kx.size()), ky.data(),
+                                    static_cast<int>(ky.size()), -1, -1, static_cast<int>(border), delta, borderValue,
+                                    nullptr));
+    return out;
+}
+
+/// gaussianBlur (include/ipf/filter.hpp:262-267).
+template <class TOut = void, class T>
+Image<detail::OutT<TOut, T>> gaussianBlur(const Image<T>& src, double sigmaX, double sigmaY = 0.0, int ksize = 0,
+                                          BorderMode border = BorderMode::Reflect101) {
+    Image<detail::OutT<TOut, T>> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_gaussian_blur(&s, &d, sigmaX, sigmaY, ksize, static_cast<int>(border), nullptr));
+    return out;
+}
+
+/// boxFilter (include/ipf/filter.hpp:206-253).
+template <class TOut = void, class T>
+Image<detail::OutT<TOut, T>> boxFilter(const Image<T>& src, int kw, int kh, bool normalize = true,
+                                       BorderMode border = BorderMode::Reflect101, double borderValue = 0.0) {
+    Image<detail::OutT<TOut, T>> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_box_filter(&s, &d, kw, kh, normalize ? 1 : 0, static_cast<int>(border), borderValue, nullptr));
+    return out;
+}
+
+/// blur (include/ipf/filter.hpp:256-259).
+template <class TOut = void, class T>
+Image<detail::OutT<TOut, T>> blur(const Image<T>& src, int ksize, BorderMode border = BorderMode::Reflect101) {
+    return boxFilter<TOut>(src, ksize, ksize, true, border);
+}
+
+/// sobel (include/ipf/filter.hpp:395-407): float output like the reference.
+template <class T>
+ImageF sobel(const Image<T>& src, int dx, int dy, int ksize = 3, double scale = 1.0,
+             BorderMode border = BorderMode::Reflect101) {
+    ImageF out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_sobel(&s, &d, dx, dy, ksize, scale, static_cast<int>(border), nullptr));
+    return out;
+}
+
+/// filter2D (include/ipf/filter.hpp:159-194).
+template <class TOut = void, class T>
+Image<detail::OutT<TOut, T>> filter2D(const Image<T>& src, const Kernel& kernel,
+                                      BorderMode border = BorderMode::Reflect101, double delta = 0.0,
+                                      Point anchor = Point(-1, -1), double borderValue = 0.0) {
+    if (kernel.channels() != 1 || kernel.empty())
+        throw ipf::Error("ipf: filter2D: kernel must be a non-empty single-channel image");
+    Image<detail::OutT<TOut, T>> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_filter2d(&s, &d, kernel.data(), kernel.width(), kernel.height(), anchor.x, anchor.y,
+                                static_cast<int>(border), delta, borderValue, nullptr));
+    return out;
+}
+
+/// medianBlur (include/ipf/filter.hpp:302-332).
+template <class T>
+Image<T> medianBlur(const Image<T>& src, int ksize, BorderMode border = BorderMode::Replicate) {
+    if (!(ksize >= 1 && ksize % 2 == 1)) throw ipf::Error("ipf: medianBlur: ksize must be odd and positive");
+    if (border == BorderMode::Constant) throw ipf::Error("ipf: medianBlur: Constant border is not supported");
+    if (src.empty() || ksize == 1) return src;
+    Image<T> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_median_blur(&s, &d, ksize, static_cast<int>(border), nullptr));
+    return out;
+}
+
+/// erode (include/ipf/morphology.hpp:112-118).
+template <class T>
+Image<T> erode(const Image<T>& src, const StructuringElement& se = getStructuringElement(MorphShape::Rect, 3),
+               int iterations = 1) {
+    if (se.channels() != 1 || se.empty())
+        throw ipf::Error("ipf: morphology: structuring element must be a non-empty single-channel mask");
+    Image<T> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_erode(&s, &d, se.data(), se.width(), se.height(), iterations, nullptr));
+    return out;
+}
+
+/// dilate (include/ipf/morphology.hpp:121-127).
+template <class T>
+Image<T> dilate(const Image<T>& src, const StructuringElement& se = getStructuringElement(MorphShape::Rect, 3),
+                int iterations = 1) {
+    if (se.channels() != 1 || se.empty())
+        throw ipf::Error("ipf: morphology: structuring element must be a non-empty single-channel mask");
+    Image<T> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_dilate(&s, &d, se.data(), se.width(), se.height(), iterations, nullptr));
+    return out;
+}
+
+}  // namespace cuda
+}  // namespace ipf
