@@ -148,6 +148,19 @@ IPFC_API int ipfc_sobel(const ipfc_image* src, ipfc_image* dst, int dx, int dy, 
 IPFC_API int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
                   int border, double delta, double border_value, void* stream);
 
+/* filter2D for callers that cannot allocate device memory (inside a custom
+ * allocator, under a framework that reserved the device's memory, in a
+ * pipeline that forbids allocation after start-up).  Same result as
+ * ipfc_filter2d, device images only; the non-zero taps are staged in a fixed
+ * 64 KB device array that the library holds on every GPU it runs on, so at
+ * most 4096 non-zero taps (larger kernels are rejected with
+ * IPFC_ERR_INVALID).  The first call on a device looks up that array's
+ * address (do it before any stream capture).  Calls share the array: calls
+ * whose kernels overlap on the GPU race on it.  No counterpart in the
+ * reference, whose CPU code allocates freely. */
+IPFC_API int ipfc_filter2d_noalloc(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax,
+                                   int ay, int border, double delta, double border_value, void* stream);
+
 /* ---- order statistics and morphology -------------------------------------- */
 
 /* medianBlur (filter.hpp:302-332): exact; Constant border is an error. */
