@@ -51,6 +51,22 @@ _SIGNATURES = {
     "ipfc_median_blur": (c_int, [IMG_P, IMG_P, c_int, c_int, c_void_p]),
     "ipfc_erode": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_void_p]),
     "ipfc_dilate": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "ipfc_batch_create": (c_int, [c_void_p]),
+    "ipfc_batch_destroy": (c_int, [c_void_p]),
+    "ipfc_batch_set_option": (c_int, [c_void_p, c_int, c_int]),
+    "ipfc_batch_add_sep_filter": (c_int, [c_void_p, IMG_P, IMG_P, c_void_p, c_int, c_void_p, c_int, c_int, c_double,
+                                          c_double]),
+    "ipfc_batch_add_gaussian_blur": (c_int, [c_void_p, IMG_P, IMG_P, c_double, c_double, c_int, c_int]),
+    "ipfc_batch_add_median_blur": (c_int, [c_void_p, IMG_P, IMG_P, c_int, c_int]),
+    "ipfc_batch_add_erode": (c_int, [c_void_p, IMG_P, IMG_P, c_void_p, c_int, c_int, c_int]),
+    "ipfc_batch_add_dilate": (c_int, [c_void_p, IMG_P, IMG_P, c_void_p, c_int, c_int, c_int]),
+    "ipfc_batch_run": (c_int, [c_void_p, c_void_p]),
+    "ipfc_batch_info": (c_int, [c_void_p, c_int, c_void_p]),
+    "ipfc_tune_get": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "ipfc_tune_set": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int]),
+    "ipfc_tune_save": (c_int, [ctypes.c_char_p]),
+    "ipfc_tune_load": (c_int, [ctypes.c_char_p, c_void_p]),
+    "ipfc_tune_clear": (c_int, []),
     "ipfc_probe_border_index": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "ipfc_probe_saturate": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p]),
 }

@@ -53,8 +53,8 @@ def _stale(target: str, deps) -> bool:
 
 def _compile(src: str, obj: str, verbose: bool) -> None:
     cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
-    if os.path.basename(src).startswith("sep_fast_"):
-        cmd.insert(1, "--split-compile=4")  # many kernels per file: compile them in parallel
+    if os.path.basename(src).startswith(("sep_fast_", "batch_")):
+        cmd.insert(1, "--split-compile=4")  # many kernels or tile functions per file: compile them in parallel
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -68,7 +68,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compiles what is stale and links the library; returns its path."""
     os.makedirs(OBJDIR, exist_ok=True)
     # the heavy instantiation files first, so the pool's tail is short
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")), key=lambda p: (not os.path.basename(p).startswith("sep_fast_"), p))
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")),
+                  key=lambda p: (not os.path.basename(p).startswith(("batch_heavy", "sep_fast_")), p))
     hdrs = _headers()
     jobs = []
     objs = []

@@ -190,7 +190,7 @@ static int finish(const ipfc_image* dst, DevView* in, DevView* out, cudaStream_t
 // Common checks: both views non-null, supported types, equal shapes, no
 // aliasing, a device present.  Returns IPFC_OK, an error, or -1 for "empty
 // image: nothing to do" (the reference returns an empty result).
-static int check_pair(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type) {
+int check_pair(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type) {
     if (!src || !dst) return set_error(IPFC_ERR_INVALID, "ipf: %s: null image", fn);
     if (src->width < 0 || src->height < 0 || src->channels < 1)
         return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid source dimensions", fn);
@@ -304,18 +304,20 @@ static unsigned long long pack_tap2(double v) {
     return ((unsigned long long)u << 32) | u;
 }
 
-// Launches the fast kernel when a fitting instantiation exists; returns
-// whether it did (e holds the launch status).
-static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const DevView& in, const DevView& out,
-                         const double* kx, int kw, const double* ky, int kh, int ax, int ay, int border, double delta,
-                         double bv, cudaStream_t s, cudaError_t* e) {
+// Argument block of the fast kernel for device views (in_ptr, in_pitch) ->
+// (out_ptr, out_pitch); false when the fast kernel does not cover the call.
+// The batch layer builds its separable items with this same function, so a
+// batched image computes exactly what the per-image call computes.
+bool make_sep_fast_args(const ipfc_image* src, const ipfc_image* dst, const void* in_ptr, long long in_pitch,
+                        void* out_ptr, long long out_pitch, const double* kx, int kw, const double* ky, int kh, int ax,
+                        int ay, int border, double delta, double bv, SepFastArgs* fp) {
     if (!sep_fast_eligible(src, kx, kw, ky, kh, ax, ay)) return false;
-    SepFastArgs f;
+    SepFastArgs& f = *fp;
     std::memset(&f, 0, sizeof(f));
-    f.src = in.ptr;
-    f.spitch = in.pitch;
-    f.dst = out.ptr;
-    f.dpitch = out.pitch;
+    f.src = in_ptr;
+    f.spitch = in_pitch;
+    f.dst = out_ptr;
+    f.dpitch = out_pitch;
     f.W = src->width;
     f.H = src->height;
     f.border = border;
@@ -326,10 +328,10 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
         f.kx2[i] = pack_tap2(kx[i]);
     }
     for (int j = 0; j < kh; ++j) f.ky2[j] = pack_tap2(ky[j]);
-    const uintptr_t op = (uintptr_t)out.ptr, ip = (uintptr_t)in.ptr;
-    f.vec_store = (op % 16 == 0 && out.pitch % 16 == 0) ? 1 : 0;
+    const uintptr_t op = (uintptr_t)out_ptr, ip = (uintptr_t)in_ptr;
+    f.vec_store = (op % 16 == 0 && out_pitch % 16 == 0) ? 1 : 0;
     const unsigned vec_align = src->dtype == IPFC_F32 ? 8u : 4u;  // 2 floats or 4 bytes per load
-    f.vec_load = (ip % vec_align == 0 && in.pitch % vec_align == 0) ? 1 : 0;
+    f.vec_load = (ip % vec_align == 0 && in_pitch % vec_align == 0) ? 1 : 0;
     // Saturation is needed unless every output provably stays inside the
     // destination range: non-negative taps bound the result between
     // delta + sum(kx)sum(ky) * min(0, lowest input) and the same with the
@@ -354,6 +356,18 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
             delta + sx * sy * hi_in < dmax + 0.25)
             f.clamp = 0;
     }
+    return true;
+}
+
+// Launches the fast kernel when a fitting instantiation exists; returns
+// whether it did (e holds the launch status).
+static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const DevView& in, const DevView& out,
+                         const double* kx, int kw, const double* ky, int kh, int ax, int ay, int border, double delta,
+                         double bv, cudaStream_t s, cudaError_t* e) {
+    SepFastArgs f;
+    if (!make_sep_fast_args(src, dst, in.ptr, in.pitch, out.ptr, out.pitch, kx, kw, ky, kh, ax, ay, border, delta, bv,
+                            &f))
+        return false;
     return sep_fast_dispatch(kw, src->channels, src->dtype, dst->dtype, f, s, e);
 }
 static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh, int ax,

@@ -1,0 +1,694 @@
+// batch.cu -- host side of the batch API (ipfc_batch_*): items, the tile
+// plan, the autotuner and the CUDA graph of a batch.
+//
+// Plan.  Every item is cut into the per-image kernels' tiles: separable
+// items into strips of the kernel's strip width by chunks of R rows,
+// median / morphology items into TX x TY tiles.  R and (TX, TY) come from
+// the autotuner, keyed on (op, taps or ksize, channels, size class).  Items
+// go to the light or heavy class (batch.cuh); within a class they are
+// ordered by estimated cost per tile, most expensive first, and each item's
+// tiles are consecutive, so the queue hands out the long tiles first and the
+// short ones fill the tail (longest-processing-time order).
+//
+// Graph.  The first run of a plan captures, on two private streams: a
+// memset of the two queue counters, then the heavy and the light persistent
+// kernels as two parallel branches.  Later runs launch the instantiated
+// graph on the caller's stream, one call for the whole batch.  The graph
+// holds the images' device addresses, so a batch is re-run on new pixels by
+// writing them into the same buffers.
+//
+// Autotuner.  For a key it has not seen on the current device, the tuner
+// builds a batch of synthetic images of the size class's representative
+// shape, runs the persistent kernel with each candidate tile shape, times
+// the runs with CUDA events and keeps the fastest.  Results live in a
+// process-wide table that ipfc_tune_save / ipfc_tune_load write to and read
+// from a text file.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "../../include/ipfc.h"
+#include "batch.cuh"
+
+namespace ipfc {
+
+int set_error(int code, const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* fn);
+int check_pair(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type);
+int gaussian_taps(double sigma, int ksize, std::vector<double>& k);
+bool make_sep_fast_args(const ipfc_image* src, const ipfc_image* dst, const void* in_ptr, long long in_pitch,
+                        void* out_ptr, long long out_pitch, const double* kx, int kw, const double* ky, int kh, int ax,
+                        int ay, int border, double delta, double bv, SepFastArgs* fp);
+cudaError_t batch_launch_light(const BatchItem*, const BatchTile*, int, unsigned*, int, size_t, cudaStream_t);
+cudaError_t batch_launch_heavy(const BatchItem*, const BatchTile*, int, unsigned*, int, size_t, cudaStream_t);
+cudaError_t batch_occupancy_light(size_t smem, int* occ);
+cudaError_t batch_occupancy_heavy(size_t smem, int* occ);
+
+cudaError_t batch_launch(int cls, const BatchItem* items, const BatchTile* tiles, int ntiles, unsigned* counter,
+                         int grid, size_t smem, cudaStream_t s) {
+    return cls == 0 ? batch_launch_light(items, tiles, ntiles, counter, grid, smem, s)
+                    : batch_launch_heavy(items, tiles, ntiles, counter, grid, smem, s);
+}
+
+cudaError_t batch_occupancy(int cls, size_t smem, int* occ) {
+    return cls == 0 ? batch_occupancy_light(smem, occ) : batch_occupancy_heavy(smem, occ);
+}
+
+namespace {
+
+// ---- autotuner table ---------------------------------------------------------
+struct TuneKey {
+    int kind, k, c, size_class;
+    bool operator<(const TuneKey& o) const {
+        if (kind != o.kind) return kind < o.kind;
+        if (k != o.k) return k < o.k;
+        if (c != o.c) return c < o.c;
+        return size_class < o.size_class;
+    }
+};
+struct TuneVal {
+    int a;  // separable: rows per tile; median / morphology: tile width (samples)
+    int b;  // median / morphology: tile height (rows)
+};
+
+constexpr int kMaxDevices = 32;
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune[kMaxDevices];
+
+// Size classes by pixel count, and the shape each class is tuned on.
+constexpr int kSizeClasses = 4;
+int size_class_of(int W, int H) {
+    const long long px = (long long)W * H;
+    return px < 65536 ? 0 : px < 524288 ? 1 : px < 2097152 ? 2 : 3;
+}
+const int kClassSide[kSizeClasses] = {192, 512, 1024, 2048};
+
+std::vector<TuneVal> candidates(int kind, int k) {
+    if (kind == kBatchSep) return {{2 * k, 0}, {4 * k, 0}, {8 * k, 0}, {16 * k, 0}};
+    return {{128, 16}, {128, 32}, {256, 16}, {256, 32}};
+}
+
+TuneVal default_val(int kind, int k) { return kind == kBatchSep ? TuneVal{8 * k, 0} : TuneVal{128, 32}; }
+
+int batch_class(int kind, int k) { return (kind == kBatchSep && k > kBatchLightMaxTaps) ? 1 : 0; }
+
+// ---- items --------------------------------------------------------------------
+struct HostItem {
+    BatchItem it;
+    int W = 0, H = 0;
+};
+
+struct Tiling {
+    int cls = 0;
+    int nx = 0, ny = 0;
+    size_t smem = 0;
+    double cost = 0;  // estimated cost of one tile (sample-operations)
+};
+
+// Applies tile parameters v to an item and describes its tiling.
+Tiling tile_item(BatchItem& it, int W, int H, TuneVal v) {
+    Tiling t;
+    t.cls = batch_class(it.kind, it.K);
+    if (it.kind == kBatchSep) {
+        const int px = batch_sep_px(it.K, it.C);
+        int rows = std::max(1, std::min(v.a, H));
+        it.u.sep.rows_per_cta = rows;
+        it.u.sep.strips = (W + px - 1) / px;
+        t.nx = it.u.sep.strips;
+        t.ny = (H + rows - 1) / rows;
+        t.smem = batch_sep_smem(it.K, it.C);
+        t.cost = (double)(2 * rows + it.K) * px * it.C * it.K;
+    } else {
+        it.tx = v.a;
+        it.ty = v.b;
+        t.nx = (W * it.C + it.tx - 1) / it.tx;
+        t.ny = (H + it.ty - 1) / it.ty;
+        if (it.kind == kBatchMedian) {
+            t.smem = median_tile_bytes(it.tx, it.ty, it.K, it.C);
+            t.cost = (double)it.tx * it.ty * it.K * it.K * 4;
+        } else {
+            const MorphCore& m = it.u.morph;
+            t.smem = morph_tile_bytes(it.tx, it.ty, m.sw, m.sh, it.C, true);
+            t.cost = (double)it.tx * (it.ty + m.sh) * (m.sw + m.sh);
+        }
+    }
+    return t;
+}
+
+// A plan in device memory: items, tiles (class 0 first), two counters.
+struct Plan {
+    BatchItem* d_items = nullptr;
+    BatchTile* d_tiles = nullptr;
+    unsigned* d_counter = nullptr;
+    int nitems = 0;
+    int ntiles[kBatchClasses] = {0, 0};
+    int tile_off[kBatchClasses] = {0, 0};
+    size_t smem[kBatchClasses] = {0, 0};
+    int grid[kBatchClasses] = {0, 0};
+    double cost[kBatchClasses] = {0, 0};
+
+    void release() {
+        if (d_items) cudaFree(d_items);
+        if (d_tiles) cudaFree(d_tiles);
+        if (d_counter) cudaFree(d_counter);
+        d_items = nullptr;
+        d_tiles = nullptr;
+        d_counter = nullptr;
+    }
+};
+
+cudaError_t make_plan(const std::vector<HostItem>& items, const std::vector<TuneVal>& vals, Plan* p) {
+    const int n = (int)items.size();
+    std::vector<BatchItem> its(n);
+    std::vector<Tiling> tl(n);
+    for (int i = 0; i < n; ++i) {
+        its[i] = items[i].it;
+        tl[i] = tile_item(its[i], items[i].W, items[i].H, vals[i]);
+    }
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        if (tl[x].cls != tl[y].cls) return tl[x].cls < tl[y].cls;
+        return tl[x].cost > tl[y].cost;
+    });
+    std::vector<BatchTile> tiles;
+    for (int c = 0; c < kBatchClasses; ++c) {
+        p->tile_off[c] = (int)tiles.size();
+        p->smem[c] = 0;
+        p->cost[c] = 0;
+        for (int i : order) {
+            if (tl[i].cls != c || items[i].W == 0 || items[i].H == 0) continue;
+            p->smem[c] = std::max(p->smem[c], tl[i].smem);
+            for (int y = 0; y < tl[i].ny; ++y)
+                for (int x = 0; x < tl[i].nx; ++x) {
+                    tiles.push_back(BatchTile{i, x, y, 0});
+                    p->cost[c] += tl[i].cost;
+                }
+        }
+        p->ntiles[c] = (int)tiles.size() - p->tile_off[c];
+    }
+    p->nitems = n;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    for (int c = 0; c < kBatchClasses && e == cudaSuccess; ++c) {
+        p->grid[c] = 0;
+        if (p->ntiles[c] == 0) continue;
+        int occ = 0;
+        e = batch_occupancy(c, p->smem[c], &occ);
+        if (e != cudaSuccess) break;
+        if (occ < 1) return cudaErrorInvalidConfiguration;
+        p->grid[c] = std::min(sms * occ, p->ntiles[c]);
+    }
+    if (e != cudaSuccess) return e;
+    if (n > 0) e = cudaMalloc((void**)&p->d_items, sizeof(BatchItem) * n);
+    if (e == cudaSuccess && !tiles.empty()) e = cudaMalloc((void**)&p->d_tiles, sizeof(BatchTile) * tiles.size());
+    if (e == cudaSuccess) e = cudaMalloc((void**)&p->d_counter, sizeof(unsigned) * kBatchClasses);
+    if (e == cudaSuccess && n > 0)
+        e = cudaMemcpy(p->d_items, its.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !tiles.empty())
+        e = cudaMemcpy(p->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) p->release();
+    return e;
+}
+
+// Enqueues one execution of a plan: counter reset, then the classes' kernels
+// (on s0, or as two parallel branches when s1 and the events are given).
+cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, cudaStream_t s1, cudaEvent_t fork, cudaEvent_t join) {
+    cudaError_t e = cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned) * kBatchClasses, s0);
+    if (e != cudaSuccess) return e;
+    const bool both = p.ntiles[0] > 0 && p.ntiles[1] > 0 && s1;
+    if (both) {
+        if ((e = cudaEventRecord(fork, s0)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s1, fork, 0)) != cudaSuccess) return e;
+    }
+    // heavy first: its tiles are the longest
+    for (int c = kBatchClasses - 1; c >= 0; --c) {
+        if (p.ntiles[c] == 0) continue;
+        cudaStream_t s = (both && c == 0) ? s1 : s0;
+        e = batch_launch(c, p.d_items, p.d_tiles + p.tile_off[c], p.ntiles[c], p.d_counter + c, p.grid[c], p.smem[c],
+                         s);
+        if (e != cudaSuccess) return e;
+    }
+    if (both) {
+        if ((e = cudaEventRecord(join, s1)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s0, join, 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Times candidate tile shapes for one key on synthetic images; returns the
+// fastest.
+cudaError_t tune_key(const TuneKey& key, const HostItem& proto, TuneVal* best) {
+    const int side = kClassSide[key.size_class];
+    const int W = side, H = side, C = key.c;
+    const long long bytes = (long long)W * H * C;
+    // enough copies to fill the device several times over
+    const int copies = (int)std::max(4LL, std::min(64LL, (64LL << 20) / std::max(1LL, bytes)));
+    unsigned char* buf = nullptr;
+    cudaError_t e = cudaMalloc((void**)&buf, (size_t)bytes * 2);
+    if (e != cudaSuccess) return e;
+    cudaStream_t s = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    e = cudaMemset(buf, 0x5a, (size_t)bytes);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1);
+    std::vector<HostItem> items((size_t)copies, proto);
+    for (HostItem& h : items) {
+        h.W = W;
+        h.H = H;
+        BatchItem& it = h.it;
+        // every copy reads the same source and writes the same destination:
+        // only the time is used
+        if (it.kind == kBatchSep) {
+            it.u.sep.src = buf;
+            it.u.sep.spitch = (long long)W * C;
+            it.u.sep.dst = buf + bytes;
+            it.u.sep.dpitch = (long long)W * C;
+            it.u.sep.W = W;
+            it.u.sep.H = H;
+            it.u.sep.vec_load = 1;
+            it.u.sep.vec_store = ((W * C) % 16 == 0) ? 1 : 0;
+        } else if (it.kind == kBatchMedian) {
+            it.u.med.src = buf;
+            it.u.med.spitch = (long long)W * C;
+            it.u.med.dst = buf + bytes;
+            it.u.med.dpitch = (long long)W * C;
+            it.u.med.W = W;
+            it.u.med.H = H;
+        } else {
+            it.u.morph.src = buf;
+            it.u.morph.spitch = (long long)W * C;
+            it.u.morph.dst = buf + bytes;
+            it.u.morph.dpitch = (long long)W * C;
+            it.u.morph.W = W;
+            it.u.morph.H = H;
+        }
+    }
+    float best_ms = 1e30f;
+    *best = default_val(key.kind, key.k);
+    for (const TuneVal& v : candidates(key.kind, key.k)) {
+        if (e != cudaSuccess) break;
+        if (key.kind != kBatchSep) {
+            const size_t need = key.kind == kBatchMedian
+                                    ? median_tile_bytes(v.a, v.b, key.k, C)
+                                    : morph_tile_bytes(v.a, v.b, proto.it.u.morph.sw, proto.it.u.morph.sh, C, true);
+            if (need > 96 * 1024) continue;
+        }
+        std::vector<TuneVal> vals((size_t)copies, v);
+        Plan p;
+        e = make_plan(items, vals, &p);
+        if (e != cudaSuccess) break;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+            e = cudaEventRecord(t0, s);
+            if (e == cudaSuccess) e = enqueue_plan(p, s, nullptr, nullptr, nullptr);
+            if (e == cudaSuccess) e = cudaEventRecord(t1, s);
+            if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+            float m = 0;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&m, t0, t1);
+            if (rep > 0) ms = std::min(ms, m);  // the first run warms up
+        }
+        p.release();
+        if (e == cudaSuccess && ms < best_ms) {
+            best_ms = ms;
+            *best = v;
+        }
+    }
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    if (s) cudaStreamDestroy(s);
+    cudaFree(buf);
+    return e;
+}
+
+bool tune_env_disabled() {
+    const char* v = std::getenv("IPFC_AUTOTUNE");
+    return v && std::strcmp(v, "0") == 0;
+}
+
+}  // namespace
+
+}  // namespace ipfc
+
+using namespace ipfc;
+
+struct ipfc_batch {
+    std::vector<HostItem> items;
+    int autotune = 1;
+    int use_graph = 1;
+    int device = -1;
+    bool planned = false;
+    Plan plan;
+    cudaStream_t st[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+
+    void drop_plan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        plan.release();
+        planned = false;
+    }
+    ~ipfc_batch() {
+        drop_plan();
+        for (int i = 0; i < 2; ++i) {
+            if (st[i]) cudaStreamDestroy(st[i]);
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        }
+    }
+};
+
+namespace {
+
+int batch_common(ipfc_batch* b, const ipfc_image* src, const ipfc_image* dst, const char* fn) {
+    if (!b) return set_error(IPFC_ERR_INVALID, "ipf: %s: null batch", fn);
+    if (!src || !dst) return set_error(IPFC_ERR_INVALID, "ipf: %s: null image", fn);
+    if (src->mem != IPFC_MEM_DEVICE || dst->mem != IPFC_MEM_DEVICE)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: batched images must be in device memory", fn);
+    if (src->dtype != IPFC_U8 || dst->dtype != IPFC_U8)
+        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: batches take uint8 images", fn);
+    if (src->channels != 1 && src->channels != 3 && src->channels != 4)
+        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: batches take 1, 3 or 4 channels", fn);
+    int rc = check_pair(src, dst, fn, false);
+    if (rc > 0) return rc;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    if (b->device < 0) b->device = dev;
+    if (b->device != dev) return set_error(IPFC_ERR_INVALID, "ipf: %s: batch belongs to device %d", fn, b->device);
+    return rc;  // 0, or -1 for an empty image
+}
+
+long long pitch_or_dense(const ipfc_image* im) {
+    return im->pitch > 0 ? im->pitch : (long long)im->width * im->channels;
+}
+
+void add_item(ipfc_batch* b, const BatchItem& it, int W, int H) {
+    HostItem h;
+    h.it = it;
+    h.W = W;
+    h.H = H;
+    b->items.push_back(h);
+    b->drop_plan();
+}
+
+int add_sep(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh,
+            int border, double delta, double bv, const char* fn) {
+    if (!kx || !ky || kw <= 0 || kh <= 0) return set_error(IPFC_ERR_INVALID, "ipf: separable filter: empty kernel");
+    if (border < IPFC_BORDER_CONSTANT || border > IPFC_BORDER_WRAP)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid border mode", fn);
+    int rc = batch_common(b, src, dst, fn);
+    if (rc > 0) return rc;
+    if (kw != kh || kw % 2 == 0 || kw < 3 || kw > kBatchMaxTaps)
+        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: batches take equal odd tap counts from 3 to %d", fn,
+                         kBatchMaxTaps);
+    BatchItem it;
+    std::memset(&it, 0, sizeof(it));
+    it.kind = kBatchSep;
+    it.K = kw;
+    it.C = src->channels;
+    if (rc == 0 && !make_sep_fast_args(src, dst, src->data, pitch_or_dense(src), dst->data, pitch_or_dense(dst), kx, kw,
+                                       ky, kh, kw / 2, kh / 2, border, delta, bv, &it.u.sep))
+        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: taps not covered by the batched kernel", fn);
+    add_item(b, it, rc == 0 ? src->width : 0, rc == 0 ? src->height : 0);
+    return IPFC_OK;
+}
+
+int plan_batch(ipfc_batch* b, const char* fn) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    if (dev >= kMaxDevices) return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: device index %d out of range", fn, dev);
+    std::vector<TuneVal> vals(b->items.size());
+    const bool tune = b->autotune && !tune_env_disabled();
+    for (size_t i = 0; i < b->items.size(); ++i) {
+        const HostItem& h = b->items[i];
+        const TuneKey key{h.it.kind, h.it.K, h.it.C, size_class_of(h.W, h.H)};
+        TuneVal v = default_val(key.kind, key.k);
+        bool found = false;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto f = g_tune[dev].find(key);
+            if (f != g_tune[dev].end()) {
+                v = f->second;
+                found = true;
+            }
+        }
+        if (!found && tune && h.W > 0) {
+            e = tune_key(key, h, &v);
+            if (e != cudaSuccess) return cuda_status(e, fn);
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune[dev][key] = v;
+        }
+        vals[i] = v;
+    }
+    e = make_plan(b->items, vals, &b->plan);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        if (!b->st[i]) e = cudaStreamCreateWithFlags(&b->st[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess && !b->ev[i]) e = cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess && b->use_graph) {
+        e = cudaStreamBeginCapture(b->st[0], cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t e2 = enqueue_plan(b->plan, b->st[0], b->st[1], b->ev[0], b->ev[1]);
+            e = cudaStreamEndCapture(b->st[0], &b->graph);
+            if (e2 != cudaSuccess) e = e2;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    }
+    if (e != cudaSuccess) {
+        b->drop_plan();
+        return cuda_status(e, fn);
+    }
+    b->planned = true;
+    return IPFC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ipfc_batch_create(ipfc_batch** out) {
+    if (!out) return set_error(IPFC_ERR_INVALID, "ipf: batch: null output pointer");
+    *out = new ipfc_batch();
+    return IPFC_OK;
+}
+
+int ipfc_batch_destroy(ipfc_batch* b) {
+    delete b;
+    return IPFC_OK;
+}
+
+int ipfc_batch_set_option(ipfc_batch* b, int option, int value) {
+    if (!b) return set_error(IPFC_ERR_INVALID, "ipf: batch: null batch");
+    if (option == IPFC_BATCH_AUTOTUNE) b->autotune = value ? 1 : 0;
+    else if (option == IPFC_BATCH_GRAPH) b->use_graph = value ? 1 : 0;
+    else return set_error(IPFC_ERR_INVALID, "ipf: batch: unknown option %d", option);
+    b->drop_plan();
+    return IPFC_OK;
+}
+
+int ipfc_batch_add_sep_filter(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, const double* kx, int kw,
+                              const double* ky, int kh, int border, double delta, double border_value) {
+    return add_sep(b, src, dst, kx, kw, ky, kh, border, delta, border_value, "sepFilter2D (batch)");
+}
+
+int ipfc_batch_add_gaussian_blur(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, double sigma_x,
+                                 double sigma_y, int ksize, int border) {
+    if (sigma_y <= 0) sigma_y = sigma_x;
+    std::vector<double> kx, ky;
+    if (gaussian_taps(sigma_x, ksize, kx)) return IPFC_ERR_INVALID;
+    if (gaussian_taps(sigma_y, ksize, ky)) return IPFC_ERR_INVALID;
+    return add_sep(b, src, dst, kx.data(), (int)kx.size(), ky.data(), (int)ky.size(), border, 0.0, 0.0,
+                   "gaussianBlur (batch)");
+}
+
+int ipfc_batch_add_median_blur(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, int ksize, int border) {
+    const char* fn = "medianBlur (batch)";
+    if (!(ksize >= 1 && ksize % 2 == 1))
+        return set_error(IPFC_ERR_INVALID, "ipf: medianBlur: ksize must be odd and positive");
+    if (border == IPFC_BORDER_CONSTANT)
+        return set_error(IPFC_ERR_INVALID, "ipf: medianBlur: Constant border is not supported");
+    if (border < IPFC_BORDER_CONSTANT || border > IPFC_BORDER_WRAP)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: invalid border mode", fn);
+    int rc = batch_common(b, src, dst, fn);
+    if (rc > 0) return rc;
+    if (ksize < 3 || ksize > 15)
+        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: batches take ksize 3 to 15 (ksize 1 is a copy)", fn);
+    BatchItem it;
+    std::memset(&it, 0, sizeof(it));
+    it.kind = kBatchMedian;
+    it.K = ksize;
+    it.C = src->channels;
+    it.u.med = MedianArgs{src->data, pitch_or_dense(src), dst->data, pitch_or_dense(dst), src->width, src->height,
+                          src->channels, ksize, border};
+    add_item(b, it, rc == 0 ? src->width : 0, rc == 0 ? src->height : 0);
+    return IPFC_OK;
+}
+
+static int batch_morph(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int sw, int sh,
+                       int iterations, bool is_min) {
+    const char* fn = is_min ? "erode (batch)" : "dilate (batch)";
+    if (!se || sw <= 0 || sh <= 0)
+        return set_error(IPFC_ERR_INVALID,
+                         "ipf: morphology: structuring element must be a non-empty single-channel mask");
+    int rc = batch_common(b, src, dst, fn);
+    if (rc > 0) return rc;
+    for (int i = 0; i < sw * sh; ++i)
+        if (!se[i]) return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: batches take all-ones (Rect) elements", fn);
+    if (iterations != 1) return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: batches take one iteration", fn);
+    if (sw > 31 || sh > 31) return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: batches take elements up to 31x31", fn);
+    BatchItem it;
+    std::memset(&it, 0, sizeof(it));
+    it.kind = kBatchMorph;
+    it.K = sw;
+    it.C = src->channels;
+    MorphCore& m = it.u.morph;
+    m.src = src->data;
+    m.spitch = pitch_or_dense(src);
+    m.dst = dst->data;
+    m.dpitch = pitch_or_dense(dst);
+    m.W = src->width;
+    m.H = src->height;
+    m.C = src->channels;
+    m.sw = sw;
+    m.sh = sh;
+    m.ax = sw / 2;
+    m.ay = sh / 2;
+    m.is_rect = 1;
+    m.is_min = is_min ? 1 : 0;
+    m.noffs = sw * sh;
+    add_item(b, it, rc == 0 ? src->width : 0, rc == 0 ? src->height : 0);
+    return IPFC_OK;
+}
+
+int ipfc_batch_add_erode(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w, int se_h,
+                         int iterations) {
+    return batch_morph(b, src, dst, se, se_w, se_h, iterations, true);
+}
+
+int ipfc_batch_add_dilate(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w,
+                          int se_h, int iterations) {
+    return batch_morph(b, src, dst, se, se_w, se_h, iterations, false);
+}
+
+int ipfc_batch_run(ipfc_batch* b, void* stream) {
+    const char* fn = "batch";
+    if (!b) return set_error(IPFC_ERR_INVALID, "ipf: batch: null batch");
+    if (b->items.empty()) return IPFC_OK;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    if (dev != b->device) return set_error(IPFC_ERR_INVALID, "ipf: batch: batch belongs to device %d", b->device);
+    if (!b->planned) {
+        int rc = plan_batch(b, fn);
+        if (rc) return rc;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->exec) {
+        e = cudaGraphLaunch(b->exec, s);
+    } else {
+        e = enqueue_plan(b->plan, s, nullptr, nullptr, nullptr);
+    }
+    return e == cudaSuccess ? IPFC_OK : cuda_status(e, fn);
+}
+
+int ipfc_batch_info(const ipfc_batch* b, int what, long long* value) {
+    if (!b || !value) return set_error(IPFC_ERR_INVALID, "ipf: batch: null argument");
+    const Plan& p = b->plan;
+    switch (what) {
+        case IPFC_BATCH_INFO_ITEMS: *value = (long long)b->items.size(); break;
+        case IPFC_BATCH_INFO_PLANNED: *value = b->planned ? 1 : 0; break;
+        case IPFC_BATCH_INFO_TILES_LIGHT: *value = p.ntiles[0]; break;
+        case IPFC_BATCH_INFO_TILES_HEAVY: *value = p.ntiles[1]; break;
+        case IPFC_BATCH_INFO_GRID_LIGHT: *value = p.grid[0]; break;
+        case IPFC_BATCH_INFO_GRID_HEAVY: *value = p.grid[1]; break;
+        case IPFC_BATCH_INFO_KERNELS: *value = (p.ntiles[0] > 0) + (p.ntiles[1] > 0); break;
+        case IPFC_BATCH_INFO_GRAPH: *value = b->exec ? 1 : 0; break;
+        default: return set_error(IPFC_ERR_INVALID, "ipf: batch: unknown info %d", what);
+    }
+    return IPFC_OK;
+}
+
+int ipfc_tune_get(int op, int k, int channels, int size_class, int* a, int* b) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= kMaxDevices) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto f = g_tune[dev].find(TuneKey{op, k, channels, size_class});
+    if (f == g_tune[dev].end()) return set_error(IPFC_ERR_INVALID, "ipf: tune: no entry");
+    if (a) *a = f->second.a;
+    if (b) *b = f->second.b;
+    return IPFC_OK;
+}
+
+int ipfc_tune_set(int op, int k, int channels, int size_class, int a, int b) {
+    if (op < kBatchSep || op > kBatchMorph || size_class < 0 || size_class >= kSizeClasses || a <= 0 ||
+        (op != kBatchSep && b <= 0))
+        return set_error(IPFC_ERR_INVALID, "ipf: tune: invalid entry");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= kMaxDevices) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[dev][TuneKey{op, k, channels, size_class}] = TuneVal{a, b};
+    return IPFC_OK;
+}
+
+int ipfc_tune_save(const char* path) {
+    if (!path) return set_error(IPFC_ERR_INVALID, "ipf: tune: null path");
+    FILE* f = std::fopen(path, "w");
+    if (!f) return set_error(IPFC_ERR_INVALID, "ipf: tune: cannot write %s", path);
+    std::fprintf(f, "# ipfc autotune table: device op k channels size_class a b\n");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int d = 0; d < kMaxDevices; ++d)
+        for (const auto& kv : g_tune[d])
+            std::fprintf(f, "%d %d %d %d %d %d %d\n", d, kv.first.kind, kv.first.k, kv.first.c, kv.first.size_class,
+                         kv.second.a, kv.second.b);
+    std::fclose(f);
+    return IPFC_OK;
+}
+
+int ipfc_tune_load(const char* path, int* count) {
+    if (!path) return set_error(IPFC_ERR_INVALID, "ipf: tune: null path");
+    FILE* f = std::fopen(path, "r");
+    if (!f) return set_error(IPFC_ERR_INVALID, "ipf: tune: cannot read %s", path);
+    char line[256];
+    int n = 0;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    while (std::fgets(line, sizeof(line), f)) {
+        if (line[0] == '#') continue;
+        int d, op, k, c, sc, a, b;
+        if (std::sscanf(line, "%d %d %d %d %d %d %d", &d, &op, &k, &c, &sc, &a, &b) != 7) continue;
+        if (d < 0 || d >= kMaxDevices || sc < 0 || sc >= kSizeClasses || a <= 0) continue;
+        g_tune[d][TuneKey{op, k, c, sc}] = TuneVal{a, b};
+        ++n;
+    }
+    std::fclose(f);
+    if (count) *count = n;
+    return IPFC_OK;
+}
+
+int ipfc_tune_clear(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int d = 0; d < kMaxDevices; ++d) g_tune[d].clear();
+    return IPFC_OK;
+}
+
+}  // extern "C"

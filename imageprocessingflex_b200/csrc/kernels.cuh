@@ -24,7 +24,8 @@ cudaError_t median_launch(int dt, const MedianArgs& a, cudaStream_t s);
 // row-major order, carried in the launch parameters.
 constexpr int kMorphMaxOffsets = 1024;
 
-struct MorphArgs {
+// Everything but the member list (all an all-ones element needs).
+struct MorphCore {
     const void* src;
     long long spitch;
     void* dst;
@@ -34,6 +35,9 @@ struct MorphArgs {
     int is_rect;
     int is_min;
     int noffs;
+};
+
+struct MorphArgs : MorphCore {
     short2 offs[kMorphMaxOffsets];
 };
 

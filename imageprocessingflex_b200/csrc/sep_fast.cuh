@@ -262,17 +262,16 @@ __device__ __noinline__ void sep_row_pass_cold(const SepFastArgs& a, const float
     sep_row_pass<K, C, Tout, G>(a, vbuf, rows_in_band, band_start, x0);
 }
 
-// ---- the kernel -------------------------------------------------------------
+// ---- one tile: a strip of PX output pixels x a chunk of a.rows_per_cta rows
+// Called by sep_fast_kernel (one tile per CTA) and by the persistent batch
+// kernel (batch.cu, tiles from a queue).  `a` may live in the parameter
+// space or in shared memory; vbuf is G::SMEM bytes of shared memory.
 template <int K, int C, typename Tin, typename Tout>
-__global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
-    sep_fast_kernel(const __grid_constant__ SepFastArgs a) {
+__device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf, int strip, int chunk) {
     constexpr int NCOL = sizeof(Tin) == 1 ? 4 : 2;
     constexpr int NP = NCOL / 2;  // accumulator pairs per ring slot
     using G = FastGeom<K, C, NCOL>;
-    extern __shared__ __align__(128) float vbuf[];  // C planes x TB rows x VWP
     const int tid = threadIdx.x;
-    const int strip = blockIdx.x % a.strips;
-    const int chunk = blockIdx.x / a.strips;
     const int x0 = strip * G::PX;                  // first output pixel of the strip
     const int r0 = chunk * a.rows_per_cta;         // first output row
     if (r0 >= a.H) return;
@@ -408,6 +407,14 @@ __global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
         });
     }
     if (band_row > 0) sep_row_pass_cold<K, C, Tout, G>(a, vbuf, band_row, band_start, x0);
+}
+
+// ---- the kernel: one tile per CTA --------------------------------------------
+template <int K, int C, typename Tin, typename Tout>
+__global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
+    sep_fast_kernel(const __grid_constant__ SepFastArgs a) {
+    extern __shared__ __align__(128) float vbuf[];  // C planes x TB rows x VWP
+    sep_fast_tile<K, C, Tin, Tout>(a, vbuf, blockIdx.x % a.strips, blockIdx.x / a.strips);
 }
 
 }  // namespace ipfc

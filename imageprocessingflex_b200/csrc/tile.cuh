@@ -18,18 +18,21 @@ __device__ __forceinline__ void load_tile(Tacc* tile, int RY, int SW, const void
                                           int C, int gq0, int gy0, int border, Tacc bv) {
     const int rowlen = W * C;
     const bool inside_x = gq0 >= 0 && gq0 + SW <= rowlen;
-    for (int r = threadIdx.y; r < RY; r += blockDim.y) {
+    // warps take rows, lanes take samples (any block shape of whole warps)
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int lane = tid & 31, nrow = (blockDim.x * blockDim.y) >> 5;
+    for (int r = tid >> 5; r < RY; r += nrow) {
         const int sy = border_index(gy0 + r, H, border);
         Tacc* dst = tile + (size_t)r * SW;
         if (sy < 0) {
-            for (int s = threadIdx.x; s < SW; s += blockDim.x) dst[s] = bv;
+            for (int s = lane; s < SW; s += 32) dst[s] = bv;
             continue;
         }
         const Tin* srow = row_ptr<Tin>(src, spitch, sy);
         if (inside_x) {
-            for (int s = threadIdx.x; s < SW; s += blockDim.x) dst[s] = static_cast<Tacc>(srow[gq0 + s]);
+            for (int s = lane; s < SW; s += 32) dst[s] = static_cast<Tacc>(srow[gq0 + s]);
         } else {
-            for (int s = threadIdx.x; s < SW; s += blockDim.x) {
+            for (int s = lane; s < SW; s += 32) {
                 const int g = gq0 + s;
                 const int idx = ((unsigned)g < (unsigned)rowlen) ? g : border_sample(g, W, C, border);
                 dst[s] = idx < 0 ? bv : static_cast<Tacc>(srow[idx]);

@@ -174,6 +174,69 @@ IPFC_API int ipfc_erode(const ipfc_image* src, ipfc_image* dst, const uint8_t* s
 IPFC_API int ipfc_dilate(const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w, int se_h, int iterations,
                 void* stream);
 
+/* ---- batches: many images, one persistent launch -------------------------
+ *
+ * No counterpart in the reference (ipf runs one call per image).  A batch
+ * collects per-image calls -- the same functions and arguments as the
+ * entry points above, on device images -- and runs them together: every
+ * image is cut into the per-image kernels' tiles, and persistent kernels
+ * walk one tile queue over all images.  The first ipfc_batch_run plans the
+ * batch (autotuned tile shapes, tile order, device tables) and captures it
+ * as a CUDA graph; later runs replay the graph on `stream`.  Each image's
+ * result is bit-identical to its per-image call.
+ *
+ * Covered: uint8 images with 1, 3 or 4 channels; separable filters and
+ * gaussianBlur with equal odd tap counts 3..25 and centred anchors;
+ * medianBlur with ksize 3..15; erode / dilate with an all-ones element up
+ * to 31x31 and one iteration.  Other calls return IPFC_ERR_UNSUPPORTED.
+ * The images must stay allocated, at the same addresses, while the batch
+ * exists; a batch is re-run on new pixels by writing them into the same
+ * buffers.  A batch belongs to the device current when its first image was
+ * added and is not safe for concurrent use from several threads. */
+typedef struct ipfc_batch ipfc_batch;
+
+enum {
+    IPFC_BATCH_AUTOTUNE = 1, /* 1 (default): tune unseen tile keys at planning; 0: built-in shapes */
+    IPFC_BATCH_GRAPH = 2     /* 1 (default): capture and replay a CUDA graph; 0: launch directly */
+};
+
+enum {
+    IPFC_BATCH_INFO_ITEMS = 0,
+    IPFC_BATCH_INFO_PLANNED = 1,
+    IPFC_BATCH_INFO_TILES_LIGHT = 2,
+    IPFC_BATCH_INFO_TILES_HEAVY = 3,
+    IPFC_BATCH_INFO_GRID_LIGHT = 4,
+    IPFC_BATCH_INFO_GRID_HEAVY = 5,
+    IPFC_BATCH_INFO_KERNELS = 6, /* persistent kernel launches per run */
+    IPFC_BATCH_INFO_GRAPH = 7
+};
+
+/* Tile keys of the autotuner: op 0 separable (k = taps), 1 median (k =
+ * ksize), 2 morphology (k = element width); size class 0..3 by pixel count
+ * (< 64Ki, < 512Ki, < 2Mi, larger).  Values: separable a = rows per tile;
+ * median / morphology a = tile width in samples, b = tile height in rows. */
+IPFC_API int ipfc_batch_create(ipfc_batch** out);
+IPFC_API int ipfc_batch_destroy(ipfc_batch* b);
+IPFC_API int ipfc_batch_set_option(ipfc_batch* b, int option, int value);
+IPFC_API int ipfc_batch_add_sep_filter(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, const double* kx, int kw,
+                                       const double* ky, int kh, int border, double delta, double border_value);
+IPFC_API int ipfc_batch_add_gaussian_blur(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, double sigma_x,
+                                          double sigma_y, int ksize, int border);
+IPFC_API int ipfc_batch_add_median_blur(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, int ksize, int border);
+IPFC_API int ipfc_batch_add_erode(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w,
+                                  int se_h, int iterations);
+IPFC_API int ipfc_batch_add_dilate(ipfc_batch* b, const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w,
+                                   int se_h, int iterations);
+IPFC_API int ipfc_batch_run(ipfc_batch* b, void* stream);
+IPFC_API int ipfc_batch_info(const ipfc_batch* b, int what, long long* value);
+IPFC_API int ipfc_tune_get(int op, int k, int channels, int size_class, int* a, int* b);
+IPFC_API int ipfc_tune_set(int op, int k, int channels, int size_class, int a, int b);
+/* Text table, one "device op k channels size_class a b" line per entry;
+ * ipfc_tune_load adds the entries it reads and stores their count. */
+IPFC_API int ipfc_tune_save(const char* path);
+IPFC_API int ipfc_tune_load(const char* path, int* count);
+IPFC_API int ipfc_tune_clear(void);
+
 /* ---- device probes of the scalar rules --------------------------------- */
 
 /* borderIndex (core.hpp:187-214) evaluated by the device code the kernels

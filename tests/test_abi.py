@@ -100,3 +100,58 @@ def test_no_cpu_fallback_without_device():
         ipf.gaussianBlur(np.zeros((4, 4), np.uint8), 1.0)
     assert e.value.status == 3
     assert "no CUDA device" in str(e.value)
+
+
+# ---- batch API: argument checks and the autotune table (no GPU needed) -------
+
+def test_batch_rejects_host_images_and_null_batch():
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    assert lib.ipfc_batch_create(ctypes.byref(h)) == 0
+    x = np.zeros((4, 4), np.uint8)
+    y = np.zeros((4, 4), np.uint8)
+    sv = _lib.IpfcImage(x.ctypes.data, 4, 4, 1, 0, 4, 0)
+    dv = _lib.IpfcImage(y.ctypes.data, 4, 4, 1, 0, 4, 0)
+    assert lib.ipfc_batch_add_gaussian_blur(h, ctypes.byref(sv), ctypes.byref(dv), 1.0, 0.0, 0, 3) == 1
+    assert "batched images must be in device memory" in lib.ipfc_last_error().decode()
+    sv.mem = dv.mem = 1
+    sv.dtype = dv.dtype = 4
+    assert lib.ipfc_batch_add_median_blur(h, ctypes.byref(sv), ctypes.byref(dv), 3, 1) == 5
+    assert "uint8" in lib.ipfc_last_error().decode()
+    assert lib.ipfc_batch_add_median_blur(None, ctypes.byref(sv), ctypes.byref(dv), 3, 1) == 1
+    v = ctypes.c_longlong(-1)
+    assert lib.ipfc_batch_info(h, 0, ctypes.byref(v)) == 0 and v.value == 0
+    assert lib.ipfc_batch_run(h, None) == 0  # nothing to do
+    assert lib.ipfc_batch_set_option(h, 99, 1) == 1
+    assert lib.ipfc_batch_destroy(h) == 0
+
+
+def test_autotune_table_round_trip(tmp_path):
+    from imageprocessingflex_b200 import batch as B
+
+    B.tune_clear()
+    assert B.tune_get(B.OP_SEP, 13, 3, 2) is None
+    B.tune_set(B.OP_SEP, 13, 3, 2, 104)
+    B.tune_set(B.OP_MEDIAN, 5, 1, 0, 256, 16)
+    with pytest.raises(ipf.Error):
+        B.tune_set(B.OP_MEDIAN, 5, 1, 9, 256, 16)
+    p = str(tmp_path / "tune.txt")
+    B.tune_save(p)
+    B.tune_clear()
+    assert B.tune_get(B.OP_SEP, 13, 3, 2) is None
+    assert B.tune_load(p) == 2
+    assert B.tune_get(B.OP_SEP, 13, 3, 2) == (104, 0)
+    assert B.tune_get(B.OP_MEDIAN, 5, 1, 0) == (256, 16)
+    B.tune_clear()
+
+
+def test_uneven_mix_is_seeded():
+    from imageprocessingflex_b200 import mix
+
+    a = mix.uneven_mix(512, seed=2024)
+    b = mix.uneven_mix(512, seed=2024)
+    assert a == b
+    ops = [it.op for it in a]
+    assert 0.4 < ops.count("gaussian") / 512 < 0.6
+    assert all(64 <= it.width <= 2048 and 64 <= it.height <= 2048 and it.channels in (1, 3, 4) for it in a)
+    assert all(0.5 <= it.sigma <= 4.0 for it in a if it.op == "gaussian")
