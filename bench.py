@@ -61,9 +61,14 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launches-only", type=int, default=0,
                     help="run this many launches of the workload on one resident image and exit (for ncu captures)")
-    ap.add_argument("--workload", default="headline", choices=["headline", "batch"],
+    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "serve"],
                     help="headline: 4K RGB gaussianBlur (the driver's line); batch: 512-image uneven mix, "
-                         "batched vs plain per-image launches")
+                         "batched vs plain per-image launches; serve: Poisson request stream through the "
+                         "continuous-batching server vs one request at a time")
+    ap.add_argument("--serve-requests", type=int, default=20000)
+    ap.add_argument("--serve-rate", type=float, default=3000.0, help="arrivals per second")
+    ap.add_argument("--serve-seed", type=int, default=77)
+    ap.add_argument("--serve-out-arena-mib", type=int, default=2048)
     ap.add_argument("--batch-images", type=int, default=512)
     ap.add_argument("--batch-seed", type=int, default=2024)
     ap.add_argument("--batch-max-side", type=int, default=2048)
@@ -484,6 +489,136 @@ def run_batch(args):
     return 0
 
 
+def run_serve(args):
+    """The served stream: `serve_requests` requests with Poisson arrivals at
+    `serve_rate`/s (area lognormal, median 1 MP, log-sd 1, clipped to
+    0.01-33 MP; aspect U[0.5, 2]; C in {1, 3}; uint8; gaussianBlur 45 %,
+    sobel 20 %, medianBlur 5x5 15 %, filter2D 15x15 20 %) from pinned host
+    memory and back, replayed open-loop through two servers on the same trace:
+      continuous -- ipfc_server defaults: 40 GiB budget, 64 slots, 4 streams,
+                    batchable requests merged into persistent launches;
+      plain      -- one request at a time (1 slot, 1 stream, no batching).
+    Latency = completion - scheduled arrival (the host's submit jitter counts
+    against the server).  Mpix/s = pixels served / (last completion - first
+    arrival)."""
+    from collections import deque
+
+    import numpy as np
+    import torch
+
+    from imageprocessingflex_b200 import mix
+    from imageprocessingflex_b200 import serve as S
+
+    reqs = mix.served_stream(args.serve_requests, rate=args.serve_rate, seed=args.serve_seed)
+    taps = mix.filter2d_taps()
+    in_bytes = 512 << 20
+    g = torch.Generator()
+    g.manual_seed(args.serve_seed)
+    arena_in = torch.randint(0, 256, (in_bytes,), dtype=torch.uint8, generator=g).pin_memory()
+    out_bytes = args.serve_out_arena_mib << 20
+    arena_out = torch.empty(out_bytes, dtype=torch.uint8).pin_memory()
+    rng = np.random.default_rng(args.serve_seed + 1)
+    offs = []
+    for r in reqs:
+        nb = r.pixels * r.channels
+        offs.append(int(rng.integers(0, (in_bytes - nb) // 256 + 1)) * 256)
+
+    def shape(r):
+        return (r.height, r.width, r.channels) if r.channels > 1 else (r.height, r.width)
+
+    def run_arm(server, trace, t0):
+        ring = deque()
+        done = {}
+        pos = 0
+
+        def collect(wait_ms=0):
+            for c in server.poll(4096, wait_ms):
+                done[c.ticket] = c
+
+        for i, r in trace:
+            nb = r.pixels * r.channels
+            src = arena_in[offs[i]:offs[i] + nb].view(shape(r))
+            ob = nb * (4 if r.op == "sobel" else 1)
+            need = (ob + 255) // 256 * 256
+            if need > out_bytes:
+                raise RuntimeError("output arena smaller than one request")
+            if pos + need > out_bytes:
+                pos = 0
+            while ring and ring[0][1] < pos + need and ring[0][2] > pos:
+                if ring[0][0] in done:
+                    ring.popleft()
+                else:
+                    collect(1)
+            raw = arena_out[pos:pos + ob]
+            dst = raw.view(torch.float32).view(shape(r)) if r.op == "sobel" else raw.view(shape(r))
+            target = t0 + r.arrival
+            while server.now() < target:
+                pass
+            if r.op == "gaussian":
+                t = server.submit("gaussian", src, dst, target, sigma_x=r.sigma, keep=False)
+            elif r.op == "sobel":
+                t = server.submit("sobel", src, dst, target, dx=r.dx, dy=r.dy, ksize=3, keep=False)
+            elif r.op == "median":
+                t = server.submit("median", src, dst, target, ksize=5, keep=False)
+            else:
+                t = server.submit("filter2d", src, dst, target, kernel=taps, keep=False)
+            ring.append((t, pos, pos + need))
+            pos += need
+            if (i & 63) == 0:
+                collect()
+        server.drain()
+        collect()
+        return done
+
+    arms = {}
+    for name, kw in (("continuous", {}), ("plain", {"max_inflight": 1, "streams": 1, "batch": False})):
+        server = S.Server(**kw)
+        warm = [(i, reqs[i]) for i in range(min(200, len(reqs)))]
+        run_arm(server, [(i, r) for i, r in warm], server.now() - reqs[0].arrival)  # warm-up: all due at once
+        torch.cuda.synchronize()
+        t0 = server.now() + 0.1
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            done = run_arm(server, list(enumerate(reqs)), t0)
+        st = server.stats()
+        server.close()
+        timed = [done[t] for t in sorted(done)]
+        if len(timed) != len(reqs):
+            raise RuntimeError(f"{name}: {len(timed)} completions for {len(reqs)} requests")
+        bad = sum(1 for c in timed if c.status != 0)
+        lat = np.array([c.latency for c in timed]) * 1e3
+        span = max(c.done for c in timed) - min(c.arrival for c in timed)
+        mpix = sum(r.pixels for r in reqs) / 1e6
+        arms[name] = {"mpix_s": round(mpix / span, 1), "requests_per_s": round(len(reqs) / span, 1),
+                      "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                      "p99_ms": round(float(np.percentile(lat, 99)), 3), "mean_ms": round(float(lat.mean()), 3),
+                      "max_ms": round(float(lat.max()), 3), "failed": bad, "span_s": round(span, 3),
+                      "max_inflight": int(st["max_inflight"]), "max_device_bytes": int(st["max_bytes"]),
+                      "batched_requests": int(st["batched"]), "batch_launches": int(st["batch_launches"]),
+                      "clocks": clk.summary()}
+    c, p = arms["continuous"], arms["plain"]
+    ops = {o: sum(1 for r in reqs if r.op == o) for o in ("gaussian", "sobel", "median", "filter2d")}
+    in_total = sum(r.pixels * r.channels for r in reqs)
+    out_total = sum(r.pixels * r.channels * (4 if r.op == "sobel" else 1) for r in reqs)
+    line = {
+        "metric": METRIC, "value": c["mpix_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": round(c["span_s"] * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded uniform 0-255)",
+        "config": {"workload": f"served stream: {len(reqs)} requests, Poisson arrivals at {args.serve_rate}/s; area "
+                               "lognormal median 1 MP log-sd 1 clipped 0.01-33 MP; aspect U[0.5,2]; C in {1,3}; "
+                               "gaussianBlur 45% (sigma~U[0.5,4]) / sobel 20% (ksize 3, f32 out) / medianBlur 5x5 "
+                               "15% / filter2D 15x15 20%; 40 GiB device budget", "seed": args.serve_seed,
+                   "ops": ops, "h2d_bytes": in_total, "d2h_bytes": out_total,
+                   "latency": "completion - scheduled arrival, host clock", "host_memory": "pinned"},
+        "latency_ms": {"p50": c["p50_ms"], "p99": c["p99_ms"]},
+        "continuous": c, "plain": p,
+        "speedup_vs_plain_mpix": round(c["mpix_s"] / p["mpix_s"], 3),
+        "e2e": {"value": c["mpix_s"], "unit": UNIT, "h2d_bytes_per_step": in_total, "d2h_bytes_per_step": out_total},
+        "clocks": c["clocks"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def launches_only(n):
     """n plain launches of the workload on one resident image, no timing:
     the program profiled by the ncu captures summarised under profiles/."""
@@ -507,6 +642,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -28,6 +28,30 @@ class IpfcImage(ctypes.Structure):
     ]
 
 
+class IpfcRequest(ctypes.Structure):
+    """Mirror of ``struct ipfc_request``."""
+
+    _fields_ = [
+        ("op", c_int), ("src", IpfcImage), ("dst", IpfcImage), ("sigma_x", c_double), ("sigma_y", c_double),
+        ("ksize", c_int), ("dx", c_int), ("dy", c_int), ("scale", c_double), ("kernel", c_void_p), ("kw", c_int),
+        ("kh", c_int), ("border", c_int), ("delta", c_double), ("border_value", c_double), ("arrival", c_double),
+    ]
+
+
+class IpfcCompletion(ctypes.Structure):
+    """Mirror of ``struct ipfc_completion``."""
+
+    _fields_ = [("ticket", ctypes.c_ulonglong), ("status", c_int), ("arrival", c_double), ("admitted", c_double),
+                ("done", c_double)]
+
+
+class IpfcServerConfig(ctypes.Structure):
+    """Mirror of ``struct ipfc_server_config``."""
+
+    _fields_ = [("device_budget_bytes", ctypes.c_size_t), ("max_inflight", c_int), ("streams", c_int),
+                ("batch", c_int)]
+
+
 IMG_P = ctypes.POINTER(IpfcImage)
 DBL_P = ctypes.POINTER(c_double)
 
@@ -67,6 +91,13 @@ _SIGNATURES = {
     "ipfc_tune_save": (c_int, [ctypes.c_char_p]),
     "ipfc_tune_load": (c_int, [ctypes.c_char_p, c_void_p]),
     "ipfc_tune_clear": (c_int, []),
+    "ipfc_server_create": (c_int, [c_void_p, ctypes.POINTER(IpfcServerConfig)]),
+    "ipfc_server_destroy": (c_int, [c_void_p]),
+    "ipfc_server_now": (c_double, [c_void_p]),
+    "ipfc_server_submit": (c_int, [c_void_p, ctypes.POINTER(IpfcRequest), c_void_p]),
+    "ipfc_server_poll": (c_int, [c_void_p, ctypes.POINTER(IpfcCompletion), c_int, c_void_p, c_int]),
+    "ipfc_server_drain": (c_int, [c_void_p, c_int]),
+    "ipfc_server_stats": (c_int, [c_void_p, c_int, c_void_p]),
     "ipfc_probe_border_index": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "ipfc_probe_saturate": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p]),
 }

@@ -36,6 +36,7 @@
 
 #include "../../include/ipfc.h"
 #include "batch.cuh"
+#include "batch_plan.h"
 
 namespace ipfc {
 
@@ -73,11 +74,6 @@ struct TuneKey {
         return size_class < o.size_class;
     }
 };
-struct TuneVal {
-    int a;  // separable: rows per tile; median / morphology: tile width (samples)
-    int b;  // median / morphology: tile height (rows)
-};
-
 constexpr int kMaxDevices = 32;
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune[kMaxDevices];
@@ -98,12 +94,6 @@ std::vector<TuneVal> candidates(int kind, int k) {
 TuneVal default_val(int kind, int k) { return kind == kBatchSep ? TuneVal{8 * k, 0} : TuneVal{128, 32}; }
 
 int batch_class(int kind, int k) { return (kind == kBatchSep && k > kBatchLightMaxTaps) ? 1 : 0; }
-
-// ---- items --------------------------------------------------------------------
-struct HostItem {
-    BatchItem it;
-    int W = 0, H = 0;
-};
 
 struct Tiling {
     int cls = 0;
@@ -135,8 +125,8 @@ Tiling tile_item(BatchItem& it, int W, int H, TuneVal v) {
             t.cost = (double)it.tx * it.ty * it.K * it.K * 4;
         } else {
             const MorphCore& m = it.u.morph;
-            t.smem = morph_tile_bytes(it.tx, it.ty, m.sw, m.sh, it.C, true);
-            t.cost = (double)it.tx * (it.ty + m.sh) * (m.sw + m.sh);
+            t.smem = morph_u8_tile_bytes(it.tx, it.ty, m.sw, m.sh, it.C);
+            t.cost = (double)it.tx * (it.ty + m.sh) * (m.sw + m.sh) / 4;
         }
     }
     return t;
@@ -144,15 +134,11 @@ Tiling tile_item(BatchItem& it, int W, int H, TuneVal v) {
 
 // A plan in device memory: items, tiles (class 0 first), two counters.
 struct Plan {
+    HostPlan host;
     BatchItem* d_items = nullptr;
     BatchTile* d_tiles = nullptr;
     unsigned* d_counter = nullptr;
-    int nitems = 0;
-    int ntiles[kBatchClasses] = {0, 0};
-    int tile_off[kBatchClasses] = {0, 0};
-    size_t smem[kBatchClasses] = {0, 0};
     int grid[kBatchClasses] = {0, 0};
-    double cost[kBatchClasses] = {0, 0};
 
     void release() {
         if (d_items) cudaFree(d_items);
@@ -164,13 +150,15 @@ struct Plan {
     }
 };
 
-cudaError_t make_plan(const std::vector<HostItem>& items, const std::vector<TuneVal>& vals, Plan* p) {
+}  // namespace
+
+void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneVal>& vals, HostPlan* p) {
     const int n = (int)items.size();
-    std::vector<BatchItem> its(n);
+    p->items.resize(n);
     std::vector<Tiling> tl(n);
     for (int i = 0; i < n; ++i) {
-        its[i] = items[i].it;
-        tl[i] = tile_item(its[i], items[i].W, items[i].H, vals[i]);
+        p->items[i] = items[i].it;
+        tl[i] = tile_item(p->items[i], items[i].W, items[i].H, vals[i]);
     }
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
@@ -178,9 +166,9 @@ cudaError_t make_plan(const std::vector<HostItem>& items, const std::vector<Tune
         if (tl[x].cls != tl[y].cls) return tl[x].cls < tl[y].cls;
         return tl[x].cost > tl[y].cost;
     });
-    std::vector<BatchTile> tiles;
+    p->tiles.clear();
     for (int c = 0; c < kBatchClasses; ++c) {
-        p->tile_off[c] = (int)tiles.size();
+        p->tile_off[c] = (int)p->tiles.size();
         p->smem[c] = 0;
         p->cost[c] = 0;
         for (int i : order) {
@@ -188,41 +176,34 @@ cudaError_t make_plan(const std::vector<HostItem>& items, const std::vector<Tune
             p->smem[c] = std::max(p->smem[c], tl[i].smem);
             for (int y = 0; y < tl[i].ny; ++y)
                 for (int x = 0; x < tl[i].nx; ++x) {
-                    tiles.push_back(BatchTile{i, x, y, 0});
+                    p->tiles.push_back(BatchTile{i, x, y, 0});
                     p->cost[c] += tl[i].cost;
                 }
         }
-        p->ntiles[c] = (int)tiles.size() - p->tile_off[c];
+        p->ntiles[c] = (int)p->tiles.size() - p->tile_off[c];
     }
-    p->nitems = n;
+}
+
+cudaError_t plan_grids(const HostPlan& p, int grid[kBatchClasses]) {
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     for (int c = 0; c < kBatchClasses && e == cudaSuccess; ++c) {
-        p->grid[c] = 0;
-        if (p->ntiles[c] == 0) continue;
+        grid[c] = 0;
+        if (p.ntiles[c] == 0) continue;
         int occ = 0;
-        e = batch_occupancy(c, p->smem[c], &occ);
+        e = batch_occupancy(c, p.smem[c], &occ);
         if (e != cudaSuccess) break;
         if (occ < 1) return cudaErrorInvalidConfiguration;
-        p->grid[c] = std::min(sms * occ, p->ntiles[c]);
+        grid[c] = std::min(sms * occ, p.ntiles[c]);
     }
-    if (e != cudaSuccess) return e;
-    if (n > 0) e = cudaMalloc((void**)&p->d_items, sizeof(BatchItem) * n);
-    if (e == cudaSuccess && !tiles.empty()) e = cudaMalloc((void**)&p->d_tiles, sizeof(BatchTile) * tiles.size());
-    if (e == cudaSuccess) e = cudaMalloc((void**)&p->d_counter, sizeof(unsigned) * kBatchClasses);
-    if (e == cudaSuccess && n > 0)
-        e = cudaMemcpy(p->d_items, its.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !tiles.empty())
-        e = cudaMemcpy(p->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) p->release();
     return e;
 }
 
-// Enqueues one execution of a plan: counter reset, then the classes' kernels
-// (on s0, or as two parallel branches when s1 and the events are given).
-cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, cudaStream_t s1, cudaEvent_t fork, cudaEvent_t join) {
-    cudaError_t e = cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned) * kBatchClasses, s0);
+cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsigned* d_counter, const HostPlan& p,
+                        const int grid[kBatchClasses], cudaStream_t s0, cudaStream_t s1, cudaEvent_t fork,
+                        cudaEvent_t join) {
+    cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * kBatchClasses, s0);
     if (e != cudaSuccess) return e;
     const bool both = p.ntiles[0] > 0 && p.ntiles[1] > 0 && s1;
     if (both) {
@@ -233,8 +214,7 @@ cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, cudaStream_t s1, cudaEv
     for (int c = kBatchClasses - 1; c >= 0; --c) {
         if (p.ntiles[c] == 0) continue;
         cudaStream_t s = (both && c == 0) ? s1 : s0;
-        e = batch_launch(c, p.d_items, p.d_tiles + p.tile_off[c], p.ntiles[c], p.d_counter + c, p.grid[c], p.smem[c],
-                         s);
+        e = batch_launch(c, d_items, d_tiles + p.tile_off[c], p.ntiles[c], d_counter + c, grid[c], p.smem[c], s);
         if (e != cudaSuccess) return e;
     }
     if (both) {
@@ -242,6 +222,42 @@ cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, cudaStream_t s1, cudaEv
         if ((e = cudaStreamWaitEvent(s0, join, 0)) != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+TuneVal tuned_or_default(int kind, int k, int c, int W, int H) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return default_val(kind, k);
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto f = g_tune[dev].find(TuneKey{kind, k, c, size_class_of(W, H)});
+    return f != g_tune[dev].end() ? f->second : default_val(kind, k);
+}
+
+namespace {
+
+cudaError_t make_plan(const std::vector<HostItem>& items, const std::vector<TuneVal>& vals, Plan* p) {
+    build_host_plan(items, vals, &p->host);
+    const HostPlan& h = p->host;
+    cudaError_t e = plan_grids(h, p->grid);
+    if (e != cudaSuccess) return e;
+    const size_t n = h.items.size();
+    if (n > 0) e = cudaMalloc((void**)&p->d_items, sizeof(BatchItem) * n);
+    if (e == cudaSuccess && !h.tiles.empty()) e = cudaMalloc((void**)&p->d_tiles, sizeof(BatchTile) * h.tiles.size());
+    if (e == cudaSuccess) e = cudaMalloc((void**)&p->d_counter, sizeof(unsigned) * kBatchClasses);
+    if (e == cudaSuccess && n > 0)
+        e = cudaMemcpy(p->d_items, h.items.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !h.tiles.empty())
+        e = cudaMemcpy(p->d_tiles, h.tiles.data(), sizeof(BatchTile) * h.tiles.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) p->release();
+    return e;
+}
+
+// Enqueues one execution of a plan: counter reset, then the classes' kernels
+// (on s0, or as two parallel branches when s1 and the events are given).
+cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, cudaStream_t s1, cudaEvent_t fork, cudaEvent_t join) {
+    return launch_plan(p.d_items, p.d_tiles, p.d_counter, p.host, p.grid, s0, s1, fork, join);
 }
 
 // Times candidate tile shapes for one key on synthetic images; returns the
@@ -300,7 +316,7 @@ cudaError_t tune_key(const TuneKey& key, const HostItem& proto, TuneVal* best) {
         if (key.kind != kBatchSep) {
             const size_t need = key.kind == kBatchMedian
                                     ? median_tile_bytes(v.a, v.b, key.k, C)
-                                    : morph_tile_bytes(v.a, v.b, proto.it.u.morph.sw, proto.it.u.morph.sh, C, true);
+                                    : morph_u8_tile_bytes(v.a, v.b, proto.it.u.morph.sw, proto.it.u.morph.sh, C);
             if (need > 96 * 1024) continue;
         }
         std::vector<TuneVal> vals((size_t)copies, v);
@@ -612,11 +628,11 @@ int ipfc_batch_info(const ipfc_batch* b, int what, long long* value) {
     switch (what) {
         case IPFC_BATCH_INFO_ITEMS: *value = (long long)b->items.size(); break;
         case IPFC_BATCH_INFO_PLANNED: *value = b->planned ? 1 : 0; break;
-        case IPFC_BATCH_INFO_TILES_LIGHT: *value = p.ntiles[0]; break;
-        case IPFC_BATCH_INFO_TILES_HEAVY: *value = p.ntiles[1]; break;
+        case IPFC_BATCH_INFO_TILES_LIGHT: *value = p.host.ntiles[0]; break;
+        case IPFC_BATCH_INFO_TILES_HEAVY: *value = p.host.ntiles[1]; break;
         case IPFC_BATCH_INFO_GRID_LIGHT: *value = p.grid[0]; break;
         case IPFC_BATCH_INFO_GRID_HEAVY: *value = p.grid[1]; break;
-        case IPFC_BATCH_INFO_KERNELS: *value = (p.ntiles[0] > 0) + (p.ntiles[1] > 0); break;
+        case IPFC_BATCH_INFO_KERNELS: *value = (p.host.ntiles[0] > 0) + (p.host.ntiles[1] > 0); break;
         case IPFC_BATCH_INFO_GRAPH: *value = b->exec ? 1 : 0; break;
         default: return set_error(IPFC_ERR_INVALID, "ipf: batch: unknown info %d", what);
     }

@@ -9,7 +9,7 @@
 // expensive tiles come first.  Each CTA of the persistent kernel then loops:
 // take the next tile index from a global counter, copy the tile's item into
 // shared memory when it changes, and run the tile body (sep_fast_tile,
-// median_tile, morph_rect_tile).  The tile bodies are the per-image kernels'
+// median_tile, morph_u8_tile).  The tile bodies are the per-image kernels'
 // own code, so a batched image is computed exactly as the per-image call
 // computes it.
 //
@@ -22,6 +22,7 @@
 
 #include "median.cuh"
 #include "morph.cuh"
+#include "morph_u8.cuh"
 #include "sep_fast.cuh"
 
 namespace ipfc {

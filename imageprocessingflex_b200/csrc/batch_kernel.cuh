@@ -25,7 +25,8 @@ static __device__ __noinline__ void batch_median_tile(int x, int y) {
 }
 
 static __device__ __noinline__ void batch_morph_tile(int x, int y) {
-    morph_rect_tile<uint8_t>(g_batch_item.u.morph, g_batch_item.tx, g_batch_item.ty, x, y, g_batch_smem);
+    morph_u8_tile(g_batch_item.u.morph, g_batch_item.tx, g_batch_item.ty, x, y,
+                  reinterpret_cast<unsigned char*>(g_batch_smem));
 }
 
 // One separable uint8 -> uint8 tile with K taps, channels from the item.

@@ -1,0 +1,52 @@
+// batch_plan.h -- host side of a batch plan, shared by the batch API
+// (batch.cu) and the request server (serve.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "batch.cuh"
+
+namespace ipfc {
+
+struct TuneVal {
+    int a;  // separable: rows per tile; median / morphology: tile width (samples)
+    int b;  // median / morphology: tile height (rows)
+};
+
+// One image and its op, with the image's size.
+struct HostItem {
+    BatchItem it;
+    int W = 0, H = 0;
+};
+
+// Items with their tile parameters applied, and the tile list: class 0
+// (light) tiles first, each class ordered by estimated cost per tile.
+struct HostPlan {
+    std::vector<BatchItem> items;
+    std::vector<BatchTile> tiles;
+    int ntiles[kBatchClasses] = {0, 0};
+    int tile_off[kBatchClasses] = {0, 0};
+    size_t smem[kBatchClasses] = {0, 0};
+    double cost[kBatchClasses] = {0, 0};
+};
+
+void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneVal>& vals, HostPlan* p);
+
+// Persistent grid of each class: resident CTAs on all SMs, at most one per
+// tile.
+cudaError_t plan_grids(const HostPlan& p, int grid[kBatchClasses]);
+
+// Enqueues the plan whose items and tiles are in device memory: resets the
+// two counters, then launches the classes on s0 (or as parallel branches
+// on s0 and s1 when s1, fork and join are given).
+cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsigned* d_counter, const HostPlan& p,
+                        const int grid[kBatchClasses], cudaStream_t s0, cudaStream_t s1, cudaEvent_t fork,
+                        cudaEvent_t join);
+
+// Tile parameters for an item: the autotuner's entry for its key on the
+// current device, else the built-in default.  Never tunes.
+TuneVal tuned_or_default(int kind, int k, int c, int W, int H);
+
+}  // namespace ipfc

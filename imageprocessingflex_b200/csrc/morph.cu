@@ -1,5 +1,6 @@
 // morph.cu -- launcher of the erosion / dilation kernel (tile code: morph.cuh).
 #include "morph.cuh"
+#include "morph_u8.cuh"
 
 namespace ipfc {
 
@@ -12,6 +13,25 @@ __global__ void __launch_bounds__(kThreads) morph_kernel(const MorphArgs a, int 
     extern __shared__ float smem[];
     if (a.is_rect) morph_rect_tile<T>(a, TX, TY, blockIdx.x, blockIdx.y, smem);
     else morph_list_tile<T>(a, TX, TY, blockIdx.x, blockIdx.y, smem);
+}
+
+// uint8 with an all-ones element: the packed-byte tile (morph_u8.cuh).
+__global__ void __launch_bounds__(kMorphU8Threads) morph_u8_kernel(const MorphCore a, int TX, int TY) {
+    extern __shared__ __align__(128) unsigned char smem_u8[];
+    morph_u8_tile(a, TX, TY, blockIdx.x, blockIdx.y, smem_u8);
+}
+
+cudaError_t morph_u8_rect(const MorphCore& a, cudaStream_t s) {
+    const int TX = 256, TY = 32;
+    const size_t smem = morph_u8_tile_bytes(TX, TY, a.sw, a.sh, a.C);
+    if (smem > 96 * 1024) return cudaErrorInvalidConfiguration;
+    static unsigned done = 0;
+    cudaError_t e = ensure_smem_attr((const void*)morph_u8_kernel, 96 * 1024, &done);
+    if (e != cudaSuccess) return e;
+    const int rowlen = a.W * a.C;
+    dim3 grid((rowlen + TX - 1) / TX, (a.H + TY - 1) / TY);
+    morph_u8_kernel<<<grid, kMorphU8Threads, smem, s>>>(a, TX, TY);
+    return cudaGetLastError();
 }
 
 template <typename T>
@@ -36,6 +56,8 @@ cudaError_t morph_typed(const MorphArgs& a, cudaStream_t s) {
 }  // namespace
 
 cudaError_t morph_launch(int dt, const MorphArgs& a, cudaStream_t s) {
+    if (dt == IPFC_U8 && a.is_rect && morph_u8_tile_bytes(256, 32, a.sw, a.sh, a.C) <= 96 * 1024)
+        return morph_u8_rect(a, s);
     switch (dt) {
         case IPFC_U8: return morph_typed<uint8_t>(a, s);
         case IPFC_U16: return morph_typed<uint16_t>(a, s);

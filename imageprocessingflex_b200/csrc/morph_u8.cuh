@@ -1,0 +1,155 @@
+// morph_u8.cuh -- erosion / dilation of uint8 images by an all-ones element:
+// the packed-byte tile used by both the per-image kernel and the batch kernel.
+//
+// Same definition as morph_rect_tile (morph.cuh, after
+// include/ipf/morphology.hpp:60-84): min (erode) or max (dilate) over the
+// sw x sh window anchored at (sw/2, sh/2); pixels outside the image never
+// count, which for an all-ones element equals padding with the identity
+// (255 for min, 0 for max) because the window always holds its in-image
+// centre.
+//
+// Memory path (the op is bound by HBM bandwidth):
+//  * staging: each source row of the tile is read with 16-byte loads from the
+//    16-byte-aligned address at or below the row's first sample, so rows of
+//    any pitch and alignment load with full-width vector loads; the row's
+//    offset into its staged copy (0..15 bytes) is kept per row.  16-byte
+//    chunks that leave the row are read byte by byte, with the identity
+//    outside the image;
+//  * compute: 4 adjacent samples per 32-bit word.  The row pass takes, for
+//    each window column i, the 4 bytes at staged offset 4t + i*C + delta
+//    (two aligned shared words and one byte permute) and folds them with a
+//    per-byte min/max; the column pass folds sh row-pass words;
+//  * store: one 32-bit store per 4 outputs when the destination address is
+//    4-byte aligned, byte stores otherwise (rows of odd pitch).
+#pragma once
+
+#include "kernels.cuh"
+
+namespace ipfc {
+
+constexpr int kMorphU8Threads = 256;
+
+__device__ __forceinline__ unsigned bmin4(unsigned a, unsigned b) { return __vminu4(a, b); }
+__device__ __forceinline__ unsigned bmax4(unsigned a, unsigned b) { return __vmaxu4(a, b); }
+
+// Bytes [s, s+4) of the staged row `w` (32-bit words), s >= 0.
+__device__ __forceinline__ unsigned staged_word(const unsigned* w, int s) {
+    const unsigned lo = w[s >> 2], hi = w[(s >> 2) + 1];
+    return __byte_perm(lo, hi, 0x3210u + 0x1111u * (unsigned)(s & 3));
+}
+
+// Geometry of one tile: TX output samples (a multiple of 4) x TY rows.
+struct MorphU8Geom {
+    int RY;  // staged rows
+    int SP;  // staged row stride (bytes, multiple of 16)
+    int TW;  // words per row-pass row (TX / 4)
+    __host__ __device__ MorphU8Geom(int TX, int TY, int sw, int sh, int C) {
+        RY = TY + sh - 1;
+        const int SWB = TX + (sw - 1) * C;
+        SP = ((SWB + 15 + 16) / 16) * 16 + 16;  // delta + samples + the last word's neighbour
+        TW = TX / 4;
+    }
+    // staged rows, row-pass rows, per-row offsets
+    __host__ __device__ size_t bytes() const {
+        return (size_t)RY * SP + (size_t)RY * TW * 4 + (size_t)RY * 4;
+    }
+};
+
+__host__ __device__ inline size_t morph_u8_tile_bytes(int TX, int TY, int sw, int sh, int C) {
+    return MorphU8Geom(TX, TY, sw, sh, C).bytes();
+}
+
+template <bool IS_MIN>
+__device__ __forceinline__ unsigned bfold(unsigned a, unsigned b) {
+    return IS_MIN ? bmin4(a, b) : bmax4(a, b);
+}
+
+template <bool IS_MIN>
+__device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, int TY, int bx, int by,
+                                                   unsigned char* smem) {
+    const MorphU8Geom g(TX, TY, a.sw, a.sh, a.C);
+    unsigned char* stage = smem;
+    unsigned* hrow = reinterpret_cast<unsigned*>(smem + (size_t)g.RY * g.SP);
+    int* delta = reinterpret_cast<int*>(hrow + (size_t)g.RY * g.TW);
+    const int C = a.C;
+    const int rowlen = a.W * C;
+    const int q0 = bx * TX, y0 = by * TY;
+    const int g0 = q0 - a.ax * C;  // global sample of staged sample 0
+    const unsigned fill = IS_MIN ? 0xffffffffu : 0u;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = kMorphU8Threads / 32;
+
+    // ---- staging
+    for (int r = warp; r < g.RY; r += nwarp) {
+        const int gy = y0 - a.ay + r;
+        uint4* dst = reinterpret_cast<uint4*>(stage + (size_t)r * g.SP);
+        const int nch = g.SP / 16;
+        if ((unsigned)gy >= (unsigned)a.H) {
+            for (int c = lane; c < nch; c += 32) dst[c] = make_uint4(fill, fill, fill, fill);
+            if (lane == 0) delta[r] = 0;
+            continue;
+        }
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(a.src) + (long long)gy * a.spitch;
+        const int d = (int)(((uintptr_t)p + (uintptr_t)(long long)g0) & 15);
+        if (lane == 0) delta[r] = d;
+        const int gc0 = g0 - d;  // global sample of the first staged chunk's first byte
+        for (int c = lane; c < nch; c += 32) {
+            const int gc = gc0 + 16 * c;
+            uint4 v;
+            if (gc >= 0 && gc + 16 <= rowlen) {
+                v = __ldg(reinterpret_cast<const uint4*>(p + gc));
+            } else {
+                unsigned w[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    unsigned x = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int gg = gc + 4 * k + b;
+                        const unsigned byte = ((unsigned)gg < (unsigned)rowlen) ? (unsigned)__ldg(p + gg) : (fill & 0xffu);
+                        x |= byte << (8 * b);
+                    }
+                    w[k] = x;
+                }
+                v = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+            dst[c] = v;
+        }
+    }
+    __syncthreads();
+
+    // ---- row pass: hrow[r][t] = fold over i of staged bytes [4t + i*C + delta_r, +4)
+    for (int it = tid; it < g.RY * g.TW; it += kMorphU8Threads) {
+        const int r = it / g.TW, t = it - r * g.TW;
+        const unsigned* w = reinterpret_cast<const unsigned*>(stage + (size_t)r * g.SP);
+        const int s0 = 4 * t + delta[r];
+        unsigned acc = staged_word(w, s0);
+        for (int i = 1; i < a.sw; ++i) acc = bfold<IS_MIN>(acc, staged_word(w, s0 + i * C));
+        hrow[it] = acc;
+    }
+    __syncthreads();
+
+    // ---- column pass and store
+    for (int it = tid; it < TY * g.TW; it += kMorphU8Threads) {
+        const int y = it / g.TW, t = it - y * g.TW;
+        const int gy = y0 + y, q = q0 + 4 * t;
+        if (gy >= a.H || q >= rowlen) continue;
+        unsigned acc = hrow[it];
+        for (int j = 1; j < a.sh; ++j) acc = bfold<IS_MIN>(acc, hrow[it + j * g.TW]);
+        unsigned char* drow = reinterpret_cast<unsigned char*>(a.dst) + (long long)gy * a.dpitch;
+        if (q + 4 <= rowlen && (((uintptr_t)(drow + q)) & 3) == 0) {
+            *reinterpret_cast<unsigned*>(drow + q) = acc;
+        } else {
+            const int n = min(4, rowlen - q);
+            for (int b = 0; b < n; ++b) drow[q + b] = (unsigned char)(acc >> (8 * b));
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void morph_u8_tile(const MorphCore& a, int TX, int TY, int bx, int by,
+                                              unsigned char* smem) {
+    if (a.is_min) morph_u8_tile_impl<true>(a, TX, TY, bx, by, smem);
+    else morph_u8_tile_impl<false>(a, TX, TY, bx, by, smem);
+}
+
+}  // namespace ipfc

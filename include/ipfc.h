@@ -237,6 +237,75 @@ IPFC_API int ipfc_tune_save(const char* path);
 IPFC_API int ipfc_tune_load(const char* path, int* count);
 IPFC_API int ipfc_tune_clear(void);
 
+/* ---- request server: continuous batching ----------------------------------
+ *
+ * No counterpart in the reference (ipf is a library of synchronous calls).
+ * A server takes filter requests -- one image and one op each, with host
+ * (preferably pinned) or device images -- and runs them on the current
+ * device from a scheduler thread: requests are admitted in arrival order as
+ * in-flight slots and device memory (a budget, from a pool the server keeps)
+ * free up, spread over several streams so that their copies and kernels
+ * overlap, and requests the batch kernels cover are merged into one
+ * persistent launch.  Each result equals the per-image call's result.
+ * Completions report the arrival, admission and completion times (seconds
+ * on the server's clock, ipfc_server_now). */
+typedef struct ipfc_server ipfc_server;
+
+enum {
+    IPFC_OP_GAUSSIAN = 0, /* gaussianBlur: sigma_x, sigma_y, ksize, border */
+    IPFC_OP_SOBEL = 1,    /* sobel: dx, dy, ksize, scale, border (dst float or int16) */
+    IPFC_OP_MEDIAN = 2,   /* medianBlur: ksize, border */
+    IPFC_OP_FILTER2D = 3, /* filter2D: kernel kw x kh (copied at submit), border, delta, border_value */
+    IPFC_OP_BOX = 4,      /* blur: ksize x ksize normalised, border */
+    IPFC_OP_ERODE = 5,    /* erode by a ksize x ksize rect */
+    IPFC_OP_DILATE = 6    /* dilate by a ksize x ksize rect */
+};
+
+typedef struct ipfc_request {
+    int op;
+    ipfc_image src;
+    ipfc_image dst;
+    double sigma_x, sigma_y;
+    int ksize;
+    int dx, dy;
+    double scale;
+    const float* kernel;
+    int kw, kh;
+    int border;
+    double delta, border_value;
+    double arrival; /* server-clock seconds; < 0: the time of submission */
+} ipfc_request;
+
+typedef struct ipfc_completion {
+    unsigned long long ticket;
+    int status; /* ipfc_status of the request */
+    double arrival, admitted, done;
+} ipfc_completion;
+
+typedef struct ipfc_server_config {
+    size_t device_budget_bytes; /* device bytes of requests in flight (default 40 GiB) */
+    int max_inflight;           /* requests in flight at once (default 64) */
+    int streams;                /* streams the work is spread over (default 4) */
+    int batch;                  /* 1 (default): merge batchable requests admitted together */
+} ipfc_server_config;
+
+enum {
+    IPFC_SERVER_STAT_GROUPS = 0,
+    IPFC_SERVER_STAT_BATCHED = 1,
+    IPFC_SERVER_STAT_BATCH_LAUNCHES = 2,
+    IPFC_SERVER_STAT_MAX_INFLIGHT = 3,
+    IPFC_SERVER_STAT_MAX_BYTES = 4,
+    IPFC_SERVER_STAT_FAILED = 5
+};
+
+IPFC_API int ipfc_server_create(ipfc_server** out, const ipfc_server_config* cfg); /* cfg NULL: defaults */
+IPFC_API int ipfc_server_destroy(ipfc_server* s); /* finishes queued and in-flight requests first */
+IPFC_API double ipfc_server_now(const ipfc_server* s);
+IPFC_API int ipfc_server_submit(ipfc_server* s, const ipfc_request* r, unsigned long long* ticket);
+IPFC_API int ipfc_server_poll(ipfc_server* s, ipfc_completion* out, int max, int* n, int wait_ms);
+IPFC_API int ipfc_server_drain(ipfc_server* s, int timeout_ms); /* < 0: no limit */
+IPFC_API int ipfc_server_stats(const ipfc_server* s, int what, double* value);
+
 /* ---- device probes of the scalar rules --------------------------------- */
 
 /* borderIndex (core.hpp:187-214) evaluated by the device code the kernels

@@ -155,3 +155,31 @@ def test_uneven_mix_is_seeded():
     assert 0.4 < ops.count("gaussian") / 512 < 0.6
     assert all(64 <= it.width <= 2048 and 64 <= it.height <= 2048 and it.channels in (1, 3, 4) for it in a)
     assert all(0.5 <= it.sigma <= 4.0 for it in a if it.op == "gaussian")
+
+
+def test_server_argument_checks():
+    lib = _lib.load()
+    r = _lib.IpfcRequest()
+    r.op = 99
+    assert lib.ipfc_server_submit(None, ctypes.byref(r), None) == 1
+    cfg = _lib.IpfcServerConfig(0, 1, 1, 1)
+    h = ctypes.c_void_p()
+    assert lib.ipfc_server_create(ctypes.byref(h), ctypes.byref(cfg)) == 1
+    assert "invalid configuration" in lib.ipfc_last_error().decode()
+    assert lib.ipfc_server_destroy(None) == 0
+
+
+def test_served_stream_is_seeded():
+    from imageprocessingflex_b200 import mix
+
+    a = mix.served_stream(4000, rate=3000.0, seed=77)
+    assert a == mix.served_stream(4000, rate=3000.0, seed=77)
+    px = np.array([r.pixels for r in a])
+    assert 1e4 * 0.99 <= px.min() and px.max() <= 33e6 * 1.01
+    assert 0.8e6 < np.median(px) < 1.25e6
+    gaps = np.diff([r.arrival for r in a])
+    assert abs(gaps.mean() - 1 / 3000.0) < 0.1 / 3000.0
+    ops = [r.op for r in a]
+    assert abs(ops.count("gaussian") / len(a) - 0.45) < 0.03
+    t = mix.filter2d_taps()
+    assert t.shape == (15, 15) and abs(float(t.sum()) - 1.0) < 1e-5
