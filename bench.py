@@ -61,7 +61,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launches-only", type=int, default=0,
                     help="run this many launches of the workload on one resident image and exit (for ncu captures)")
-    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "serve"],
+    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "serve", "filter2d"],
                     help="headline: 4K RGB gaussianBlur (the driver's line); batch: 512-image uneven mix, "
                          "batched vs plain per-image launches; serve: Poisson request stream through the "
                          "continuous-batching server vs one request at a time")
@@ -619,6 +619,114 @@ def run_serve(args):
     return 0
 
 
+def run_filter2d(args):
+    """Dense filter2D on 4096x4096x1 (uint8 uniform 0-255 and float U[0,1)),
+    seeded N(0,1) taps normalised to sum 1, 15x15 and 31x31, Reflect101: the
+    FP32 CUDA-core form against the split-precision tcgen05 form, each timed
+    with CUDA events over `steps` launches on resident images (inputs larger
+    than L2 are not needed: the op is compute-bound; two image pairs rotate).
+    Errors against the FP64 oracle are measured on a 1024x512 crop of the same
+    kind of image with the same taps."""
+    import numpy as np
+    import torch
+
+    import imageprocessingflex_b200 as ipf
+    import oracle
+    from imageprocessingflex_b200 import _lib, mix
+
+    lib = _lib.load()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.Stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    N = 4096
+    tf = {}
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    tc_peak = float(peaks.get("bf16_tflops", 1590.0))
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # FP32 FMA pipe, TFLOP/s at the max clock
+    orc = oracle.restatement()
+    results = []
+    for dt in ("u8", "f32"):
+        g = torch.Generator(device=dev)
+        g.manual_seed(3)
+        if dt == "u8":
+            srcs = [torch.randint(0, 256, (N, N), generator=g, device=dev, dtype=torch.int32).to(torch.uint8)
+                    for _ in range(2)]
+            code, es = 0, 1
+        else:
+            srcs = [torch.rand((N, N), generator=g, device=dev, dtype=torch.float32) for _ in range(2)]
+            code, es = 4, 4
+        dsts = [torch.empty_like(x) for x in srcs]
+        views = [(_lib.IpfcImage(x.data_ptr(), N, N, 1, code, N * es, 1), _lib.IpfcImage(y.data_ptr(), N, N, 1, code,
+                                                                                           N * es, 1))
+                 for x, y in zip(srcs, dsts)]
+        crop = oracle.random_image(1024, 512, 1, np.uint8 if dt == "u8" else np.float32, 11)
+        for kk in (15, 31):
+            taps = mix.filter2d_taps(kk, seed=1000 + kk)
+            tp = taps.ctypes.data
+            row = {"dtype": dt, "taps": f"{kk}x{kk}"}
+            for form, fn in (("fp32", lib.ipfc_filter2d_fp32), ("split", lib.ipfc_filter2d_split)):
+                def step(i):
+                    sv, dv = views[i % 2]
+                    rc = fn(ctypes.byref(sv), ctypes.byref(dv), tp, kk, kk, -1, -1, BORDER_REFLECT101, 0.0, 0.0, sptr)
+                    if rc:
+                        raise RuntimeError(lib.ipfc_last_error().decode())
+                steps = max(2, args.steps if form == "split" else min(args.steps, 5))
+                for i in range(args.warmup):
+                    step(i)
+                stream.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for i in range(steps):
+                    step(i)
+                e1.record(stream)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1) / steps
+                flops = 2.0 * N * N * kk * kk
+                row[form] = {"ms": round(ms, 4), "mpix_s": round(N * N / (ms / 1e3) / 1e6, 1),
+                             "tflops": round(flops / (ms / 1e3) / 1e12, 2)}
+            row["speedup_split_vs_fp32"] = round(row["fp32"]["ms"] / row["split"]["ms"], 3)
+            row["split"]["frac_of_bf16_peak"] = round(row["split"]["tflops"] / tc_peak, 4)
+            row["fp32"]["frac_of_fp32_fma_peak"] = round(row["fp32"]["tflops"] / fp32_peak, 4)
+            # errors against the FP64 oracle (crop)
+            ref = orc.filter2d(crop, taps, 3, 0.0, (-1, -1), 0.0, np.float64)
+            for form in ("fp32", "split"):
+                got = ipf.filter2D(crop, taps, form=form, dtype=np.float32).astype(np.float64)
+                err = np.abs(got - ref)
+                row[form]["err_vs_fp64_max"] = float(f"{err.max():.4g}")
+                row[form]["err_vs_fp64_mean"] = float(f"{err.mean():.4g}")
+            if dt == "u8":
+                want = orc.filter2d(crop, taps, 3)
+                got = ipf.filter2D(crop, taps, form="split")
+                d = np.abs(got.astype(int) - want.astype(int))
+                row["split"]["u8_max_lsb"] = int(d.max())
+                row["split"]["u8_mismatch_rate"] = float(f"{(d > 0).mean():.4g}")
+                row["saturated_fraction"] = float(f"{((want == 0) | (want == 255)).mean():.4g}")
+            results.append(row)
+            tf[(dt, kk)] = row
+    head = tf[("u8", 31)]
+    line = {
+        "metric": METRIC, "value": head["split"]["mpix_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["split"]["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8 pixels exact in f16, taps f16 hi+lo, f32 accumulate",
+        "data": "synthetic (seeded uniform)",
+        "config": {"workload": "filter2D 4096x4096x1, dense N(0,1) taps normalised to sum 1, Reflect101; FP32 "
+                               "CUDA-core form vs split-precision tcgen05 form", "value_is": "u8 31x31 split Mpix/s",
+                   "flops_per_launch": "2*W*H*kw*kh (counted once, not per hi/lo product)"},
+        "cases": results,
+        "roofline": {"bound": "tensor", "achieved": head["split"]["tflops"], "peak": tc_peak, "unit": "TFLOP/s",
+                     "frac": head["split"]["frac_of_bf16_peak"], "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (dense, burst)"},
+        "gpu_launches": (args.steps + args.warmup) * 8,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def launches_only(n):
     """n plain launches of the workload on one resident image, no timing:
     the program profiled by the ncu captures summarised under profiles/."""
@@ -644,6 +752,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "filter2d":
+        return run_filter2d(args)
     return run_ours(args)
 
 

@@ -70,6 +70,10 @@ _SIGNATURES = {
     "ipfc_sobel": (c_int, [IMG_P, IMG_P, c_int, c_int, c_int, c_double, c_int, c_void_p]),
     "ipfc_filter2d": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_double,
                               c_void_p]),
+    "ipfc_filter2d_fp32": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_double,
+                                   c_void_p]),
+    "ipfc_filter2d_split": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_double,
+                                    c_void_p]),
     "ipfc_filter2d_noalloc": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_int, c_int, c_double,
                                       c_double, c_void_p]),
     "ipfc_median_blur": (c_int, [IMG_P, IMG_P, c_int, c_int, c_void_p]),

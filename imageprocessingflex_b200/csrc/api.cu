@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/ipfc.h"
+#include "filter2d_tc.cuh"
 #include "kernels.cuh"
 #include "sep_fast_launch.cuh"
 #include "tma.cuh"
@@ -274,6 +275,11 @@ int deriv_taps(int order, int ksize, std::vector<double>& k) {
 
 // Kernel selection for separable filters: IPFC_SEP_PATH=generic forces the
 // generic fused/two-pass kernels (used to check one form against the other).
+bool filter2d_tc_eligible(int sdt, int ddt, int C, int kw, int kh);
+cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spitch, void* dst, long long dpitch, int W,
+                               int H, const float* taps, int kw, int kh, int ax, int ay, int border, float delta,
+                               float bv, cudaStream_t s);
+
 static int sep_path_mode() {
     static int mode = -1;
     if (mode < 0) {
@@ -585,9 +591,31 @@ int ipfc_box_filter(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int 
     return rc;
 }
 
-int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
-                  int border, double delta, double border_value, void* stream) {
-    const char* fn = "filter2D";
+}  // extern "C"
+
+namespace ipfc {
+
+// filter2D forms: the FP32 CUDA-core kernel (filter2d.cu) and the
+// split-precision tensor-core kernel (filter2d_tc.cu).
+enum F2DForm { kF2DAuto = 0, kF2DFp32 = 1, kF2DSplit = 2 };
+
+// Automatic choice: the FP32 CUDA-core form; IPFC_F2D_PATH=split selects the
+// tensor-core form wherever it applies, =fp32 pins the CUDA-core form.
+static int f2d_auto_form(const ipfc_image* src, const ipfc_image* dst, int kw, int kh) {
+    static int forced = -1;
+    if (forced < 0) {
+        const char* v = std::getenv("IPFC_F2D_PATH");
+        forced = (v && std::strcmp(v, "fp32") == 0) ? kF2DFp32 : (v && std::strcmp(v, "split") == 0) ? kF2DSplit : 0;
+    }
+    const bool tc_ok = filter2d_tc_eligible(src->dtype, dst->dtype, src->channels, kw, kh);
+    if (forced == kF2DSplit && tc_ok) return kF2DSplit;
+    if (forced == kF2DFp32) return kF2DFp32;
+    (void)tc_ok;
+    return kF2DFp32;
+}
+
+static int run_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
+                        int border, double delta, double border_value, void* stream, int form, const char* fn) {
     if (!kernel || kw <= 0 || kh <= 0)
         return set_error(IPFC_ERR_INVALID, "ipf: filter2D: kernel must be a non-empty single-channel image");
     if (ax < 0) ax = kw / 2;
@@ -598,6 +626,12 @@ int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, i
     int rc = check_pair(src, dst, fn, false);
     if (rc == -1) return IPFC_OK;
     if (rc) return rc;
+    if (form == kF2DSplit && !filter2d_tc_eligible(src->dtype, dst->dtype, src->channels, kw, kh))
+        return set_error(IPFC_ERR_UNSUPPORTED,
+                         "ipf: %s: the tensor-core form takes single-channel uint8 (to uint8, uint16, int16, float) "
+                         "or float (to float) images and kernels up to %dx%d",
+                         fn, kTcMaxKw, kTcMaxKh);
+    if (form == kF2DAuto) form = f2d_auto_form(src, dst, kw, kh);
     cudaStream_t s = (cudaStream_t)stream;
     std::vector<float4> taps;
     for (int j = 0; j < kh; ++j)
@@ -629,6 +663,13 @@ int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, i
     a.spitch = in.pitch;
     a.dst = out.ptr;
     a.dpitch = out.pitch;
+    if (form == kF2DSplit) {
+        cudaError_t e = filter2d_tc_launch(src->dtype, dst->dtype, in.ptr, in.pitch, out.ptr, out.pitch, a.W, a.H,
+                                           kernel, kw, kh, ax, ay, border, (float)delta, (float)border_value, s);
+        rc = finish(dst, &in, &out, s, fn);
+        if (e != cudaSuccess) return cuda_status(e, fn);
+        return rc;
+    }
     float4* dtaps = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&dtaps, sizeof(float4) * (taps.size() ? taps.size() : 1), s);
     if (e == cudaSuccess && !taps.empty())
@@ -639,6 +680,25 @@ int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, i
     rc = finish(dst, &in, &out, s, fn);
     if (e != cudaSuccess) return cuda_status(e, fn);
     return rc;
+}
+
+}  // namespace ipfc
+
+extern "C" {
+
+int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
+                  int border, double delta, double border_value, void* stream) {
+    return run_filter2d(src, dst, kernel, kw, kh, ax, ay, border, delta, border_value, stream, kF2DAuto, "filter2D");
+}
+
+int ipfc_filter2d_fp32(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
+                       int border, double delta, double border_value, void* stream) {
+    return run_filter2d(src, dst, kernel, kw, kh, ax, ay, border, delta, border_value, stream, kF2DFp32, "filter2D");
+}
+
+int ipfc_filter2d_split(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
+                        int border, double delta, double border_value, void* stream) {
+    return run_filter2d(src, dst, kernel, kw, kh, ax, ay, border, delta, border_value, stream, kF2DSplit, "filter2D");
 }
 
 int ipfc_median_blur(const ipfc_image* src, ipfc_image* dst, int ksize, int border, void* stream) {

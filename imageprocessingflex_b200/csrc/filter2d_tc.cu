@@ -1,0 +1,412 @@
+// filter2d_tc.cu -- filter2D on the 5th-generation tensor cores (tcgen05):
+// split-precision FP16 operands, FP32 accumulation in tensor memory.
+//
+// Geometry and the GEMM form are in filter2d_tc.cuh.  One persistent CTA per
+// SM (256 threads) walks the 128 x 64 output tiles:
+//  1. once per CTA: both B parts (taps hi and lo, banded, in the shared
+//     layout) are copied from global memory, 64 tensor-memory columns are
+//     allocated (4 accumulators of 16 fp32 columns x 128 lanes) and the MMA
+//     barrier is initialised;
+//  2. per tile, all threads stage the transposed source tile: 8 source rows
+//     x 4 pixels per work item, borders resolved at load, pixels converted
+//     to FP16 (uint8: exact; float: hi and lo parts under a per-tile power of
+//     two), stored as 16-byte rows of K-major core matrices;
+//  3. one thread issues the MMAs -- 4 groups x kw tap columns x Kt/16 K steps
+//     x 2 (uint8) or 3 (float) precision terms -- and commits them to the
+//     barrier;
+//  4. all threads wait on the barrier (bounded), read the accumulators with
+//     tcgen05.ld (warp w reads lanes 32 (w mod 4) .. +31, half the columns
+//     each), scale, add delta, saturate_cast and store 128-pixel row runs.
+// Every wait is bounded; a timeout records kErrTcWait in the device error
+// word, ends the tile loop on all threads, and the CTA still frees its
+// tensor memory after a last bounded wait for the MMAs in flight.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/ipfc.h"
+#include "common.cuh"
+#include "filter2d_tc.cuh"
+#include "tma.cuh"
+
+namespace ipfc {
+
+int set_error(int code, const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* fn);
+unsigned* device_error_word();
+cudaError_t ensure_smem_attr(const void* func, int bytes, unsigned* done_mask);
+
+constexpr unsigned kErrTcWait = 0x201u;  // the MMA completion barrier never fired
+
+struct F2DTcArgs {
+    const void* src;
+    long long spitch;
+    void* dst;
+    long long dpitch;
+    int W, H, border;
+    float delta, bv;
+    int kw, kh, ax, ay;
+    float tap_unscale;  // 2^-s
+    float tap_sum;      // sum of the taps (FP64 on the host, rounded once)
+    int tiles_x, ntiles;
+    const uint4* btab;  // 2 B parts, shared layout
+    unsigned* err;
+};
+
+namespace {
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(addr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Two accumulator sets of kTcGroups x 16 columns: the hi x hi products
+// ("main") and the small hi x lo / lo x hi correction products, which are
+// added once, in FP32, when the results are read.
+constexpr int kTmemCols = 128;
+constexpr int kCorrCol = 64;
+
+// Source samples of one work item: 8 rows x 4 pixels starting at image
+// (gy0, gx0), borders resolved (-1: the Constant border value).
+template <typename Tin>
+__device__ __forceinline__ void load_item(const F2DTcArgs& a, int gy0, int gx0, float (&v)[8][4]) {
+    const bool cols_in = gx0 >= 0 && gx0 + 4 <= a.W;
+    int cx[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) cx[c] = cols_in ? gx0 + c : border_index(gx0 + c, a.W, a.border);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int sy = border_index(gy0 + j, a.H, a.border);
+        if (sy < 0) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) v[j][c] = a.bv;
+            continue;
+        }
+        const Tin* row = row_ptr<Tin>(a.src, a.spitch, sy);
+        if constexpr (sizeof(Tin) == 1) {
+            if (cols_in && (((uintptr_t)(row + gx0)) & 3) == 0) {
+                const unsigned w = __ldg(reinterpret_cast<const unsigned*>(row + gx0));
+#pragma unroll
+                for (int c = 0; c < 4; ++c) v[j][c] = (float)((w >> (8 * c)) & 0xffu);
+                continue;
+            }
+        } else {
+            if (cols_in && (((uintptr_t)(row + gx0)) & 15) == 0) {
+                const float4 q = __ldg(reinterpret_cast<const float4*>(row + gx0));
+                v[j][0] = q.x;
+                v[j][1] = q.y;
+                v[j][2] = q.z;
+                v[j][3] = q.w;
+                continue;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[j][c] = cx[c] < 0 ? a.bv : (float)__ldg(row + cx[c]);
+    }
+}
+
+__device__ __forceinline__ unsigned h2_bits(__half2 h) { return *reinterpret_cast<unsigned*>(&h); }
+
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid_constant__ F2DTcArgs a) {
+    constexpr bool FSRC = sizeof(Tin) == 4;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const TcGeom g(a.kw, a.kh, a.ax, a.ay, FSRC);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + g.offBar);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + g.offBar + 8);
+    float* red = reinterpret_cast<float*>(sm + g.offBar + 16);  // 8 warp maxima, 8 minima, scale, centre
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // ---- once per CTA: B parts, barrier, tensor memory
+    {
+        const int n16 = 2 * g.bytesB / 16;
+        uint4* b = reinterpret_cast<uint4*>(sm);
+        for (int i = tid; i < n16; i += kTcThreads) b[i] = __ldg(a.btab + i);
+    }
+    if (tid == 0) mbar_init(bar, 1);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *tslot;
+    const uint32_t sm_base = smem_u32(sm);
+    unsigned phase = 0;
+    bool ok = true;
+    const int nq = g.XR / 4, ns = g.KR / 8, items = nq * ns;
+
+    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        const int tx0 = (t % a.tiles_x) * kTcM, ty0 = (t / a.tiles_x) * kTcRows;
+        const int gx_base = tx0 - g.axa, gy_base = ty0 - a.ay;
+
+        // ---- 2. stage the transposed tile
+        // Operands are centred: uint8 pixels minus 128 (exact in FP16); float
+        // tiles about the middle of their range, scaled by a power of two so
+        // that the largest centred magnitude lies in [2^14, 2^15).  The
+        // epilogue adds centre * sum(taps) back.
+        float escale = 1.f, unscale = a.tap_unscale, centre = 128.f;
+        if constexpr (FSRC) {
+            float mx = -3.4e38f, mn = 3.4e38f;
+            for (int it = tid; it < items; it += kTcThreads) {
+                float v[8][4];
+                load_item<Tin>(a, gy_base + 8 * (it / nq), gx_base + 4 * (it % nq), v);
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        mx = fmaxf(mx, v[j][c]);
+                        mn = fminf(mn, v[j][c]);
+                    }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            }
+            if (lane == 0) {
+                red[warp] = mx;
+                red[8 + warp] = mn;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                float gmx = -3.4e38f, gmn = 3.4e38f;
+                for (int w = 0; w < kTcThreads / 32; ++w) {
+                    gmx = fmaxf(gmx, red[w]);
+                    gmn = fminf(gmn, red[8 + w]);
+                }
+                const float c = 0.5f * gmx + 0.5f * gmn;
+                const float r = fmaxf(gmx - c, c - gmn);
+                int ex = 0;
+                if (r > 0.f && r <= 3.0e38f) {
+                    frexpf(r, &ex);  // r = f 2^ex, f in [0.5, 1)
+                    ex = 15 - ex;
+                    ex = ex < -120 ? -120 : (ex > 120 ? 120 : ex);
+                }
+                red[16] = (float)ex;
+                red[17] = (c == c && fabsf(c) <= 3.0e38f) ? c : 0.f;
+            }
+            __syncthreads();
+            const int ex = (int)red[16];
+            centre = red[17];
+            escale = ldexpf(1.f, ex);
+            unscale = a.tap_unscale * ldexpf(1.f, -ex);
+        }
+        const float offset = fmaf(centre, a.tap_sum, a.delta);
+        for (int it = tid; it < items; it += kTcThreads) {
+            const int q = it % nq, s = it / nq;
+            float v[8][4];
+            load_item<Tin>(a, gy_base + 8 * s, gx_base + 4 * q, v);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                unsigned hi[4], lo[4];
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const float x0 = (v[2 * p][c] - centre) * escale, x1 = (v[2 * p + 1][c] - centre) * escale;
+                    const __half2 h = __floats2half2_rn(x0, x1);
+                    hi[p] = h2_bits(h);
+                    if constexpr (FSRC) {
+                        const float2 hf = __half22float2(h);
+                        lo[p] = h2_bits(__floats2half2_rn(x0 - hf.x, x1 - hf.y));
+                    }
+                }
+                const int off = g.a_off(4 * q + c, 8 * s);
+                *reinterpret_cast<uint4*>(sm + g.offA + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                if constexpr (FSRC)
+                    *reinterpret_cast<uint4*>(sm + g.offA + g.bytesA + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+            }
+        }
+        fence_async_smem();
+        __syncthreads();
+
+        // ---- 3. MMAs
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = sm_base + g.offA, a1 = a0 + g.bytesA, b0 = sm_base, b1 = sm_base + g.bytesB;
+            for (int gi = 0; gi < kTcGroups; ++gi) {
+                const uint32_t dm = tbase + (uint32_t)(kTcN * gi), dc = dm + (uint32_t)kCorrCol;
+                uint32_t acc = 0;
+                for (int i = 0; i < a.kw; ++i) {
+                    const uint32_t ash = (uint32_t)(i + g.axa - a.ax) * 16u;
+                    for (int ks = 0; ks < g.Kt / 16; ++ks) {
+                        const uint32_t aoff = (uint32_t)(2 * gi + 2 * ks) * (uint32_t)g.lboA + ash;
+                        const uint32_t boff = (uint32_t)(i * g.bytesBi + 2 * ks * 256);
+                        const uint64_t da0 = tc_smem_desc(a0 + aoff, g.lboA, 128);
+                        const uint64_t db0 = tc_smem_desc(b0 + boff, 256, 128);
+                        const uint64_t db1 = tc_smem_desc(b1 + boff, 256, 128);
+                        tc_mma(dm, da0, db0, acc);
+                        tc_mma(dc, da0, db1, acc);
+                        if constexpr (FSRC) tc_mma(dc, tc_smem_desc(a1 + aoff, g.lboA, 128), db0, 1u);
+                        acc = 1u;
+                    }
+                }
+            }
+            tc_commit(bar);
+        }
+
+        // ---- 4. wait, read the accumulators, store
+        ok = mbar_wait(bar, phase, a.err, kErrTcWait);
+        ok = __syncthreads_and(ok) != 0;
+        if (!ok) break;
+        phase ^= 1u;
+        tc_fence_after();
+        const int m = 32 * (warp & 3) + lane;
+        const int x = tx0 + m;
+        const int c0 = (warp >> 2) * 32;  // first accumulator column of this warp
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float v[16], w[16];
+            const uint32_t ta = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(c0 + 16 * h);
+            tmem_ld16(ta, v);
+            tmem_ld16(ta + (uint32_t)kCorrCol, w);
+            if (x < a.W) {
+#pragma unroll
+                for (int n = 0; n < 16; ++n) {
+                    const int y = ty0 + c0 + 16 * h + n;
+                    if (y < a.H)
+                        row_ptr_mut<Tout>(a.dst, a.dpitch, y)[x] = sat_from_f<Tout>(fmaf(v[n] + w[n], unscale, offset));
+                }
+            }
+        }
+        tc_fence_before();
+        __syncthreads();  // accumulators and the staged tile are free again
+    }
+
+    // ---- teardown: no MMA may still run when the columns are freed
+    if (!ok && tid == 0) mbar_wait(bar, phase, a.err, kErrTcWait);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
+}
+
+bool tc_supported(int sdt, int ddt) {
+    return (sdt == IPFC_U8 && (ddt == IPFC_U8 || ddt == IPFC_F32 || ddt == IPFC_I16 || ddt == IPFC_U16)) ||
+           (sdt == IPFC_F32 && ddt == IPFC_F32);
+}
+
+template <typename Tin, typename Tout>
+cudaError_t tc_launch_typed(const F2DTcArgs& a, const TcGeom& g, cudaStream_t s) {
+    static unsigned done = 0;
+    cudaError_t e = ensure_smem_attr((const void*)filter2d_tc_kernel<Tin, Tout>, 227 * 1024, &done);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const int grid = a.ntiles < sms ? a.ntiles : sms;
+    if (g.alloc > 227 * 1024) return cudaErrorInvalidConfiguration;
+    filter2d_tc_kernel<Tin, Tout><<<grid, kTcThreads, g.alloc, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// Builds the two B parts (taps hi and lo, scaled by 2^s) in the shared layout.
+void tc_build_b(const TcGeom& g, const float* taps, std::vector<__half>& out, float* tap_unscale) {
+    double mx = 0;
+    for (int j = 0; j < g.kh; ++j)
+        for (int i = 0; i < g.kw; ++i) mx = std::fmax(mx, std::fabs((double)taps[(size_t)j * g.kw + i]));
+    int ex = 0;
+    if (mx > 0) {
+        std::frexp(mx, &ex);
+        ex = 15 - ex;  // max |w| * 2^s in [2^14, 2^15)
+    }
+    *tap_unscale = (float)std::ldexp(1.0, -ex);
+    out.assign((size_t)g.bytesB, __float2half(0.f));  // 2 parts x bytesB / 2 halves
+    for (int i = 0; i < g.kw; ++i)
+        for (int n = 0; n < kTcN; ++n)
+            for (int j = 0; j < g.kh; ++j) {
+                const int k = n + j;
+                const double w = std::ldexp((double)taps[(size_t)j * g.kw + i], ex);
+                const __half hi = __double2half(w);
+                const __half lo = __double2half(w - (double)__half2float(hi));
+                const size_t o = (size_t)g.b_off(i, n, k) / 2;
+                out[o] = hi;
+                out[(size_t)g.bytesB / 2 + o] = lo;
+            }
+}
+
+bool filter2d_tc_eligible(int sdt, int ddt, int C, int kw, int kh) {
+    return C == 1 && tc_supported(sdt, ddt) && kw >= 1 && kh >= 1 && kw <= kTcMaxKw && kh <= kTcMaxKh;
+}
+
+// Launches the tensor-core form; taps are the dense kw x kh kernel (host).
+cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spitch, void* dst, long long dpitch, int W,
+                               int H, const float* taps, int kw, int kh, int ax, int ay, int border, float delta,
+                               float bv, cudaStream_t s) {
+    const TcGeom g(kw, kh, ax, ay, sdt == IPFC_F32);
+    std::vector<__half> bt;
+    F2DTcArgs a;
+    std::memset(&a, 0, sizeof(a));
+    tc_build_b(g, taps, bt, &a.tap_unscale);
+    double tsum = 0;
+    for (int k = 0; k < kw * kh; ++k) tsum += (double)taps[k];
+    a.tap_sum = (float)tsum;
+    uint4* dbt = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&dbt, bt.size() * sizeof(__half), s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(dbt, bt.data(), bt.size() * sizeof(__half), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        a.src = src;
+        a.spitch = spitch;
+        a.dst = dst;
+        a.dpitch = dpitch;
+        a.W = W;
+        a.H = H;
+        a.border = border;
+        a.delta = delta;
+        a.bv = bv;
+        a.kw = kw;
+        a.kh = kh;
+        a.ax = ax;
+        a.ay = ay;
+        a.tiles_x = (W + kTcM - 1) / kTcM;
+        a.ntiles = a.tiles_x * ((H + kTcRows - 1) / kTcRows);
+        a.btab = dbt;
+        a.err = device_error_word();
+        if (sdt == IPFC_F32) e = tc_launch_typed<float, float>(a, g, s);
+        else if (ddt == IPFC_U8) e = tc_launch_typed<uint8_t, uint8_t>(a, g, s);
+        else if (ddt == IPFC_U16) e = tc_launch_typed<uint8_t, uint16_t>(a, g, s);
+        else if (ddt == IPFC_I16) e = tc_launch_typed<uint8_t, int16_t>(a, g, s);
+        else e = tc_launch_typed<uint8_t, float>(a, g, s);
+    }
+    cudaFreeAsync(dbt, s);
+    return e;
+}
+
+}  // namespace ipfc

@@ -1,0 +1,105 @@
+// filter2d_tc.cuh -- geometry of the tensor-core (tcgen05) form of filter2D:
+// shared-memory layouts, descriptors and tile sizes, shared by the kernel
+// (filter2d_tc.cu) and host-side checks.
+//
+// The correlation out[y][x] = sum_{j,i} w[j][i] P[y + j - ay][x + i - ax]
+// (include/ipf/filter.hpp:159-194, single channel) becomes, for one CTA tile
+// of 128 output pixels (x = tx0 + m) by NG x 16 output rows
+// (y = ty0 + 16 g + n), NG groups of MMAs
+//
+//   D_g[m][n] = sum_i sum_k A_{g,i}[m][k] * B_i[n][k]          (M=128, N=16)
+//   A_{g,i}[m][k] = T[m + sh_i][16 g + k],   sh_i = i + (axa - ax)
+//   B_i[n][k]     = w[k - n][i]  for 0 <= k - n < kh, else 0
+//
+// where T[x'][r] = P[ty0 - ay + r][tx0 - axa + x'] is the source tile stored
+// transposed (x' major, source rows r contiguous) and axa = ax rounded up to
+// a multiple of 4 (so staged pixel quads start 4-aligned in the image).
+// Both operands are K-major without swizzle: 8 x 16-byte core matrices,
+// rows 16 bytes apart, so shifting A by one pixel (the tap offset i) is a
+// 16-byte move of the descriptor's start address -- one staged tile serves
+// all kw horizontal offsets, and the vertical taps live in the banded B.
+//
+// Split precision: uint8 pixels are exact in FP16; float pixels are split
+// into hi = fp16(p * 2^e) and lo = fp16(p * 2^e - hi) with a per-tile power
+// of two 2^e; taps into hi = fp16(w * 2^s), lo = fp16(w * 2^s - hi).  The
+// products hi*hi + hi*lo + lo*hi (lo*lo dropped; uint8: A*hi + A*lo) are
+// accumulated in FP32 in tensor memory and scaled back by 2^-(e+s).  Pixels
+// are centred first (uint8: p - 128, exact; float: about the tile's mid-range)
+// and hi*hi goes to its own accumulator, apart from the small correction
+// products, which keeps the accumulators small and their rounding low.
+#pragma once
+
+#include <stdint.h>
+
+namespace ipfc {
+
+constexpr int kTcM = 128;          // output pixels per tile (MMA M)
+constexpr int kTcN = 16;           // output rows per MMA group (MMA N)
+constexpr int kTcGroups = 4;       // MMA groups per tile
+constexpr int kTcRows = kTcN * kTcGroups;
+constexpr int kTcThreads = 256;
+constexpr int kTcMaxKw = 32;
+constexpr int kTcMaxKh = 33;
+
+struct TcGeom {
+    int kw, kh, ax, ay;
+    int axa;     // ax rounded up to a multiple of 4
+    int Kt;      // K of one group's window (>= kh + 15, multiple of 16)
+    int XR;      // staged pixels per tile row (multiple of 8)
+    int KR;      // staged source rows (multiple of 8)
+    int lboA;    // bytes between A's 8-row K slabs (= XR * 16)
+    int bytesA;  // one A part
+    int bytesBi; // one tap column of one B part
+    int bytesB;  // one B part (kw columns)
+    int partsA;  // 1 (uint8) or 2 (float hi, lo)
+    int offA;    // shared offsets
+    int offBar;
+    int smem;   // bytes the layout uses
+    int alloc;  // bytes allocated (>= smem)
+
+    __host__ __device__ TcGeom(int kw_, int kh_, int ax_, int ay_, bool float_src) {
+        kw = kw_;
+        kh = kh_;
+        ax = ax_;
+        ay = ay_;
+        axa = (ax + 3) / 4 * 4;
+        Kt = (kh + 15 + 15) / 16 * 16;
+        XR = (kTcM + kw - 1 + (axa - ax) + 7) / 8 * 8;
+        KR = 16 * (kTcGroups - 1) + Kt;
+        lboA = XR * 16;
+        bytesA = (KR / 8) * lboA;
+        bytesBi = (Kt / 8) * 256;
+        bytesB = kw * bytesBi;
+        partsA = float_src ? 2 : 1;
+        offA = 2 * bytesB;
+        offBar = offA + partsA * bytesA;
+        smem = offBar + 128;
+        // Allocation: also covers every address an A descriptor could reach
+        // with its two strides read the other way round (8-row groups LBO
+        // apart, K halves 128 bytes apart), so no operand read can leave the
+        // CTA's shared memory whatever the layout interpretation.
+        const int a_last = (partsA - 1) * bytesA + (2 * (kTcGroups - 1) + Kt / 8 - 2) * lboA +
+                           (kw - 1 + (axa - ax)) * 16;
+        const int swapped_end = offA + a_last + 15 * lboA + 7 * 16 + 128 + 16;
+        alloc = swapped_end > smem ? swapped_end : smem;
+        alloc = (alloc + 127) / 128 * 128;
+    }
+    // byte offset of T[x'][r] in an A part
+    __host__ __device__ int a_off(int xr, int r) const { return (r >> 3) * lboA + xr * 16 + (r & 7) * 2; }
+    // byte offset of B_i[n][k] in a B part
+    __host__ __device__ int b_off(int i, int n, int k) const {
+        return i * bytesBi + (k >> 3) * 256 + (n >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2;
+    }
+};
+
+// tcgen05 shared-memory descriptor: no swizzle, K-major, version 1.
+__host__ __device__ inline uint64_t tc_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3fff) | ((uint64_t)((lbo >> 4) & 0x3fff) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3fff) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16: D f32, A and B f16, both K-major,
+// N = 16, M = 128.
+constexpr uint32_t kTcIdesc = (1u << 4) | ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+
+}  // namespace ipfc

@@ -249,17 +249,23 @@ def sobel(src, dx, dy, ksize=3, scale=1.0, border=BorderMode.Reflect101, dtype=n
     return dst
 
 
+_F2D_ENTRY = {"auto": "ipfc_filter2d", "fp32": "ipfc_filter2d_fp32", "split": "ipfc_filter2d_split"}
+
+
 def filter2D(src, kernel, border=BorderMode.Reflect101, delta=0.0, anchor=(-1, -1), borderValue=0.0, dtype=None,
-             stream=None):
-    """filter2D (filter.hpp:159-194): correlation with float32 taps (kh, kw)."""
+             stream=None, form="auto"):
+    """filter2D (filter.hpp:159-194): correlation with float32 taps (kh, kw).
+
+    ``form``: "auto" (the library's choice), "fp32" (CUDA cores, FP32) or
+    "split" (tcgen05 tensor cores, FP16 hi + lo operands, FP32 accumulation)."""
     lib = _lib.load()
+    entry = getattr(lib, _F2D_ENTRY[form])
     k = np.ascontiguousarray(np.asarray(kernel, dtype=np.float32))
     if k.ndim != 2 or k.size == 0:
         raise Error("ipf: filter2D: kernel must be a non-empty single-channel image")
     sv, keep, dst, dv = _pair(src, dtype)
-    _check(lib.ipfc_filter2d(ctypes.byref(sv), ctypes.byref(dv), k.ctypes.data, k.shape[1], k.shape[0],
-                             int(anchor[0]), int(anchor[1]), int(border), float(delta), float(borderValue),
-                             _stream_of(src, stream)))
+    _check(entry(ctypes.byref(sv), ctypes.byref(dv), k.ctypes.data, k.shape[1], k.shape[0], int(anchor[0]),
+                 int(anchor[1]), int(border), float(delta), float(borderValue), _stream_of(src, stream)))
     del keep
     return dst
 

@@ -158,6 +158,23 @@ IPFC_API int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* 
  * address (do it before any stream capture).  Calls share the array: calls
  * whose kernels overlap on the GPU race on it.  No counterpart in the
  * reference, whose CPU code allocates freely. */
+/* The two forms of filter2D behind ipfc_filter2d, for callers that choose:
+ *  ipfc_filter2d_fp32  -- CUDA cores, FP32 accumulation, every channel count
+ *                         and element type;
+ *  ipfc_filter2d_split -- tcgen05 tensor cores: uint8 pixels exact in FP16 or
+ *                         float pixels split into FP16 hi + lo (with a per-tile
+ *                         power-of-two scale), taps split into FP16 hi + lo,
+ *                         FP32 accumulation.  Single-channel images, uint8 to
+ *                         uint8 / uint16 / int16 / float or float to float,
+ *                         kernels up to 32 x 33; otherwise
+ *                         IPFC_ERR_UNSUPPORTED.  Non-finite float pixels give
+ *                         NaN where the reference's skipped zero taps would not.
+ * Same arguments and checks as ipfc_filter2d (filter.hpp:159-194). */
+IPFC_API int ipfc_filter2d_fp32(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax,
+                                int ay, int border, double delta, double border_value, void* stream);
+IPFC_API int ipfc_filter2d_split(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax,
+                                 int ay, int border, double delta, double border_value, void* stream);
+
 IPFC_API int ipfc_filter2d_noalloc(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax,
                                    int ay, int border, double delta, double border_value, void* stream);
 
