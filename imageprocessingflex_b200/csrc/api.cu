@@ -599,8 +599,11 @@ namespace ipfc {
 // split-precision tensor-core kernel (filter2d_tc.cu).
 enum F2DForm { kF2DAuto = 0, kF2DFp32 = 1, kF2DSplit = 2 };
 
-// Automatic choice: the FP32 CUDA-core form; IPFC_F2D_PATH=split selects the
-// tensor-core form wherever it applies, =fp32 pins the CUDA-core form.
+// Automatic choice: the tensor-core form for single-channel uint8 sources
+// and kernels of 15 x 15 taps and more (many times faster than the FP32 form,
+// with uint8 pixels exact and an error against the FP64 reference on a par
+// with it), the FP32 CUDA-core form otherwise.  IPFC_F2D_PATH=split selects
+// the tensor-core form wherever it applies, =fp32 pins the CUDA-core form.
 static int f2d_auto_form(const ipfc_image* src, const ipfc_image* dst, int kw, int kh) {
     static int forced = -1;
     if (forced < 0) {
@@ -610,8 +613,7 @@ static int f2d_auto_form(const ipfc_image* src, const ipfc_image* dst, int kw, i
     const bool tc_ok = filter2d_tc_eligible(src->dtype, dst->dtype, src->channels, kw, kh);
     if (forced == kF2DSplit && tc_ok) return kF2DSplit;
     if (forced == kF2DFp32) return kF2DFp32;
-    (void)tc_ok;
-    return kF2DFp32;
+    return (tc_ok && src->dtype == IPFC_U8 && kw * kh >= 225) ? kF2DSplit : kF2DFp32;
 }
 
 static int run_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,

@@ -2,24 +2,26 @@
 // split-precision FP16 operands, FP32 accumulation in tensor memory.
 //
 // Geometry and the GEMM form are in filter2d_tc.cuh.  One persistent CTA per
-// SM (256 threads) walks the 128 x 64 output tiles:
-//  1. once per CTA: both B parts (taps hi and lo, banded, in the shared
-//     layout) are copied from global memory, 64 tensor-memory columns are
-//     allocated (4 accumulators of 16 fp32 columns x 128 lanes) and the MMA
-//     barrier is initialised;
-//  2. per tile, all threads stage the transposed source tile: 8 source rows
-//     x 4 pixels per work item, borders resolved at load, pixels converted
-//     to FP16 (uint8: exact; float: hi and lo parts under a per-tile power of
-//     two), stored as 16-byte rows of K-major core matrices;
-//  3. one thread issues the MMAs -- 4 groups x kw tap columns x Kt/16 K steps
-//     x 2 (uint8) or 3 (float) precision terms -- and commits them to the
-//     barrier;
-//  4. all threads wait on the barrier (bounded), read the accumulators with
-//     tcgen05.ld (warp w reads lanes 32 (w mod 4) .. +31, half the columns
-//     each), scale, add delta, saturate_cast and store 128-pixel row runs.
+// SM walks the 128 x 64 output tiles with 8 worker warps and one MMA warp:
+//  1. once per CTA: B (taps hi and lo side by side, banded, in the shared
+//     layout) is copied from global memory, 256 tensor-memory columns are
+//     allocated (two accumulator sets) and the barriers initialised;
+//  2. per tile, the workers stage the transposed source tile into one of two
+//     A buffers: 8 source rows x 4 pixels per work item, borders resolved at
+//     load, pixels centred and converted to FP16 (uint8: exact; float: hi
+//     and lo parts under a per-tile power of two), stored as 16-byte rows of
+//     K-major core matrices;
+//  3. one thread of the MMA warp issues the tile's MMAs -- 4 groups x kw tap
+//     columns x Kt/16 K steps, each one N = 32 MMA (hi and lo taps) plus,
+//     for float sources, one N = 16 MMA (lo pixels x hi taps) -- into one of
+//     two accumulator sets and commits them to a barrier;
+//  4. the workers read the previous tile's accumulators with tcgen05.ld
+//     (warp w reads lanes 32 (w mod 4) .. +31, half the columns each), add
+//     the correction set, scale, add the offset, saturate_cast and store
+//     128-pixel row runs -- while the tensor cores work on the next tile.
 // Every wait is bounded; a timeout records kErrTcWait in the device error
-// word, ends the tile loop on all threads, and the CTA still frees its
-// tensor memory after a last bounded wait for the MMAs in flight.
+// word and ends the loops, and the CTA frees its tensor memory only after a
+// last bounded wait for every MMA it issued.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -52,7 +54,7 @@ struct F2DTcArgs {
     float tap_unscale;  // 2^-s
     float tap_sum;      // sum of the taps (FP64 on the host, rounded once)
     int tiles_x, ntiles;
-    const uint4* btab;  // 2 B parts, shared layout
+    const uint4* btab;  // B in the shared layout
     unsigned* err;
 };
 
@@ -62,13 +64,14 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
     const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
-        "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
 }
 
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
@@ -89,11 +92,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Two accumulator sets of kTcGroups x 16 columns: the hi x hi products
-// ("main") and the small hi x lo / lo x hi correction products, which are
-// added once, in FP32, when the results are read.
-constexpr int kTmemCols = 128;
-constexpr int kCorrCol = 64;
+// Tensor memory: two accumulator sets (double buffer, 256 columns apart).
+// Group g of a set owns columns 64 g .. 64 g + 63: tap columns i of even
+// index accumulate at +0, odd ones at +32, each as the hi x hi products
+// ("main", 16 columns) followed by the small hi x lo / lo x hi correction
+// products (16 columns).  Splitting the sum four ways keeps every
+// accumulator small (its rounding is relative to its magnitude); the four
+// are added once, in FP32, when the results are read.
+constexpr int kTmemCols = 512;
+constexpr int kSetCols = 256;
+constexpr int kCorrCol = 16;
+constexpr int kOddCol = 32;
 
 // Source samples of one work item: 8 rows x 4 pixels starting at image
 // (gy0, gx0), borders resolved (-1: the Constant border value).
@@ -136,23 +145,209 @@ __device__ __forceinline__ void load_item(const F2DTcArgs& a, int gy0, int gx0, 
 
 __device__ __forceinline__ unsigned h2_bits(__half2 h) { return *reinterpret_cast<unsigned*>(&h); }
 
+// Barrier among the staging / epilogue warps only (the issuer warp is not
+// part of it).
+__device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kTcWorkers) : "memory"); }
+
+// Per-tile scaling of the staged operands and of the results.
+struct TileScale {
+    float escale;   // applied to centred pixels before the FP16 split
+    float centre;   // subtracted from pixels
+    float unscale;  // 2^-(e+s): accumulator -> result
+    float offset;   // centre * sum(taps) + delta
+};
+
+// Stages tile (tx0, ty0) into A buffer `abuf` (all worker threads).
+template <typename Tin>
+__device__ __forceinline__ TileScale stage_tile(const F2DTcArgs& a, const TcGeom& g, unsigned char* sm, int abuf,
+                                                float* red, int tx0, int ty0, int wtid) {
+    constexpr bool FSRC = sizeof(Tin) == 4;
+    const int nq = g.XR / 4, ns = g.KR / 8, items = nq * ns;
+    const int gx_base = tx0 - g.axa, gy_base = ty0 - a.ay;
+    // Operands are centred: uint8 pixels minus 128 (exact in FP16); float
+    // tiles about the middle of their range, scaled by a power of two so
+    // that the largest centred magnitude lies in [2^14, 2^15).  The epilogue
+    // adds centre * sum(taps) back.
+    TileScale ts{1.f, 128.f, a.tap_unscale, 0.f};
+    if constexpr (FSRC) {
+        const int warp = wtid >> 5, lane = wtid & 31;
+        float mx = -3.4e38f, mn = 3.4e38f;
+        for (int it = wtid; it < items; it += kTcWorkers) {
+            float v[8][4];
+            load_item<Tin>(a, gy_base + 8 * (it / nq), gx_base + 4 * (it % nq), v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    mx = fmaxf(mx, v[j][c]);
+                    mn = fminf(mn, v[j][c]);
+                }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        }
+        if (lane == 0) {
+            red[warp] = mx;
+            red[8 + warp] = mn;
+        }
+        workers_sync();
+        if (wtid == 0) {
+            float gmx = -3.4e38f, gmn = 3.4e38f;
+            for (int w = 0; w < kTcWorkers / 32; ++w) {
+                gmx = fmaxf(gmx, red[w]);
+                gmn = fminf(gmn, red[8 + w]);
+            }
+            const float c = 0.5f * gmx + 0.5f * gmn;
+            const float r = fmaxf(gmx - c, c - gmn);
+            int ex = 0;
+            if (r > 0.f && r <= 3.0e38f) {
+                frexpf(r, &ex);  // r = f 2^ex, f in [0.5, 1)
+                ex = 15 - ex;
+                ex = ex < -120 ? -120 : (ex > 120 ? 120 : ex);
+            }
+            red[16] = (float)ex;
+            red[17] = (c == c && fabsf(c) <= 3.0e38f) ? c : 0.f;
+        }
+        workers_sync();
+        const int ex = (int)red[16];
+        ts.centre = red[17];
+        ts.escale = ldexpf(1.f, ex);
+        ts.unscale = a.tap_unscale * ldexpf(1.f, -ex);
+    }
+    ts.offset = fmaf(ts.centre, a.tap_sum, a.delta);
+    unsigned char* A0 = sm + g.a_buf(abuf, 0);
+    unsigned char* A1 = sm + g.a_buf(abuf, FSRC ? 1 : 0);
+    for (int it = wtid; it < items; it += kTcWorkers) {
+        const int q = it % nq, s = it / nq;
+        float v[8][4];
+        load_item<Tin>(a, gy_base + 8 * s, gx_base + 4 * q, v);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            unsigned hi[4], lo[4];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const float x0 = (v[2 * p][c] - ts.centre) * ts.escale, x1 = (v[2 * p + 1][c] - ts.centre) * ts.escale;
+                const __half2 h = __floats2half2_rn(x0, x1);
+                hi[p] = h2_bits(h);
+                if constexpr (FSRC) {
+                    const float2 hf = __half22float2(h);
+                    lo[p] = h2_bits(__floats2half2_rn(x0 - hf.x, x1 - hf.y));
+                }
+            }
+            const int off = g.a_off(4 * q + c, 8 * s);
+            *reinterpret_cast<uint4*>(A0 + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            if constexpr (FSRC) *reinterpret_cast<uint4*>(A1 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        }
+    }
+    return ts;
+}
+
+// Reads accumulator set `set` of tile (tx0, ty0) and stores the results
+// (all worker threads; warp w reads TMEM lanes 32 (w mod 4) .. +31).
+template <typename Tout>
+__device__ __forceinline__ void epilogue_tile(const F2DTcArgs& a, uint32_t tbase, int set, int tx0, int ty0,
+                                              const TileScale& ts, int wtid) {
+    const int warp = wtid >> 5, lane = wtid & 31;
+    const int x = tx0 + 32 * (warp & 3) + lane;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int gi = 2 * (warp >> 2) + h;  // warps 0-3: groups 0, 1; warps 4-7: groups 2, 3
+        float v[16], w[16], u[16], z[16];
+        const uint32_t ta = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(set * kSetCols + 64 * gi);
+        tmem_ld16(ta, v);
+        tmem_ld16(ta + (uint32_t)kCorrCol, w);
+        if (a.kw > 1) {
+            tmem_ld16(ta + (uint32_t)kOddCol, u);
+            tmem_ld16(ta + (uint32_t)(kOddCol + kCorrCol), z);
+        } else {
+#pragma unroll
+            for (int n = 0; n < 16; ++n) u[n] = z[n] = 0.f;
+        }
+        if (x < a.W) {
+#pragma unroll
+            for (int n = 0; n < 16; ++n) {
+                const int y = ty0 + kTcN * gi + n;
+                if (y < a.H) {
+                    const float acc = (v[n] + w[n]) + (u[n] + z[n]);
+                    row_ptr_mut<Tout>(a.dst, a.dpitch, y)[x] = sat_from_f<Tout>(fmaf(acc, ts.unscale, ts.offset));
+                }
+            }
+        }
+    }
+}
+
+// Issues the MMAs of one tile from A buffer `abuf` into accumulator set
+// `set` (one thread).  Descriptors advance by adding (offset >> 4) to the
+// start-address field, which never carries: shared addresses stay below
+// 2^18 bytes.
+template <bool FSRC>
+__device__ __forceinline__ void issue_tile(const F2DTcArgs& a, const TcGeom& g, uint32_t sm_base, uint32_t tbase,
+                                           int abuf, int set) {
+    const uint64_t da0 = tc_smem_desc(sm_base + (uint32_t)g.a_buf(abuf, 0), (uint32_t)g.lboA, 128);
+    const uint64_t da1 = tc_smem_desc(sm_base + (uint32_t)g.a_buf(abuf, FSRC ? 1 : 0), (uint32_t)g.lboA, 128);
+    (void)da1;
+    const uint64_t db = tc_smem_desc(sm_base, 512, 128);  // 32 rows: hi taps, then lo taps
+    const int ksteps = g.Kt / 16;
+    const uint32_t lbo16 = (uint32_t)g.lboA >> 4;
+    constexpr uint32_t id32 = tc_idesc(2 * kTcN), id16 = tc_idesc(kTcN);
+    for (int gi = 0; gi < kTcGroups; ++gi) {
+        const uint32_t d0 = tbase + (uint32_t)(set * kSetCols + 64 * gi);
+        uint32_t first[2] = {0u, 0u};  // accumulate flags of the even and odd accumulators
+        for (int i = 0; i < a.kw; ++i) {
+            const uint32_t dm = d0 + (uint32_t)((i & 1) * kOddCol), dc = dm + (uint32_t)kCorrCol;
+            const uint32_t ash16 = (uint32_t)(i + g.axa - a.ax);  // 16-byte rows
+            const uint32_t bi16 = (uint32_t)(i * g.bytesBi) >> 4;
+            uint32_t acc = first[i & 1];
+#pragma unroll 4
+            for (int ks = 0; ks < ksteps; ++ks) {
+                const uint32_t ao = (uint32_t)(2 * gi + 2 * ks) * lbo16 + ash16;
+                const uint32_t bo = bi16 + (uint32_t)(ks * 64);  // 2 slabs of 512 bytes
+                tc_mma(dm, da0 + ao, db + bo, id32, acc);        // hi and lo taps: main and correction
+                if constexpr (FSRC) tc_mma(dc, da1 + ao, db + bo, id16, 1u);  // lo pixels x hi taps
+                acc = 1u;
+            }
+            first[i & 1] = 1u;
+        }
+    }
+}
+
+// Pipeline (per CTA, tiles t_0, t_1, ... of this CTA; buffer b = k mod 2):
+//   workers: stage t_k into A[b], arrive full[b]; then read out t_{k-1}
+//            (wait mma[b^1], tcgen05.ld, store), arrive tfree[b^1];
+//   issuer:  wait full[b] and (k >= 2) tfree[b], issue t_k's MMAs into
+//            accumulator set b, commit to mma[b].
+// So staging of t_k and the read-out of t_{k-1} overlap the MMAs of t_{k-1}
+// and t_k.  A[b] is free again once mma[b] of t_{k-2} has fired, which the
+// workers saw in the read-out of t_{k-2}.
 template <typename Tin, typename Tout>
 __global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid_constant__ F2DTcArgs a) {
     constexpr bool FSRC = sizeof(Tin) == 4;
     extern __shared__ __align__(1024) unsigned char sm[];
     const TcGeom g(a.kw, a.kh, a.ax, a.ay, FSRC);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + g.offBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + g.offBar + 8);
-    float* red = reinterpret_cast<float*>(sm + g.offBar + 16);  // 8 warp maxima, 8 minima, scale, centre
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm + g.offBar);   // [2]
+    uint64_t* mma = full + 2;                                        // [2]
+    uint64_t* tfree = full + 4;                                      // [2]
+    uint64_t* drained = full + 6;                                    // teardown
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + g.offBar + 64);
+    float* red = reinterpret_cast<float*>(sm + g.offBar + 80);       // 8 maxima, 8 minima, scale, centre
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    // ---- once per CTA: B parts, barrier, tensor memory
+    // ---- once per CTA: B parts, barriers, tensor memory
     {
-        const int n16 = 2 * g.bytesB / 16;
+        const int n16 = g.bytesB / 16;
         uint4* b = reinterpret_cast<uint4*>(sm);
         for (int i = tid; i < n16; i += kTcThreads) b[i] = __ldg(a.btab + i);
     }
-    if (tid == 0) mbar_init(bar, 1);
+    if (tid == 0) {
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&full[b], kTcWorkers);
+            mbar_init(&mma[b], 1);
+            mbar_init(&tfree[b], kTcWorkers);
+        }
+        mbar_init(drained, 1);
+    }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                      "r"(kTmemCols)
@@ -166,153 +361,65 @@ __global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid
     tc_fence_after();
     const uint32_t tbase = *tslot;
     const uint32_t sm_base = smem_u32(sm);
-    unsigned phase = 0;
-    bool ok = true;
-    const int nq = g.XR / 4, ns = g.KR / 8, items = nq * ns;
 
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const int tx0 = (t % a.tiles_x) * kTcM, ty0 = (t / a.tiles_x) * kTcRows;
-        const int gx_base = tx0 - g.axa, gy_base = ty0 - a.ay;
-
-        // ---- 2. stage the transposed tile
-        // Operands are centred: uint8 pixels minus 128 (exact in FP16); float
-        // tiles about the middle of their range, scaled by a power of two so
-        // that the largest centred magnitude lies in [2^14, 2^15).  The
-        // epilogue adds centre * sum(taps) back.
-        float escale = 1.f, unscale = a.tap_unscale, centre = 128.f;
-        if constexpr (FSRC) {
-            float mx = -3.4e38f, mn = 3.4e38f;
-            for (int it = tid; it < items; it += kTcThreads) {
-                float v[8][4];
-                load_item<Tin>(a, gy_base + 8 * (it / nq), gx_base + 4 * (it % nq), v);
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        mx = fmaxf(mx, v[j][c]);
-                        mn = fminf(mn, v[j][c]);
-                    }
+    if (warp == kTcWorkers / 32) {
+        // ---- the MMA issuer
+        if (lane == 0) {
+            int k = 0;
+            for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++k) {
+                const int b = k & 1;
+                if (!mbar_wait(&full[b], (unsigned)(k >> 1) & 1u, a.err, kErrTcWait)) break;
+                if (k >= 2 && !mbar_wait(&tfree[b], (unsigned)((k - 2) >> 1) & 1u, a.err, kErrTcWait)) break;
+                tc_fence_after();
+                issue_tile<FSRC>(a, g, sm_base, tbase, b, b);
+                tc_commit(&mma[b]);
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-            }
-            if (lane == 0) {
-                red[warp] = mx;
-                red[8 + warp] = mn;
-            }
-            __syncthreads();
-            if (tid == 0) {
-                float gmx = -3.4e38f, gmn = 3.4e38f;
-                for (int w = 0; w < kTcThreads / 32; ++w) {
-                    gmx = fmaxf(gmx, red[w]);
-                    gmn = fminf(gmn, red[8 + w]);
-                }
-                const float c = 0.5f * gmx + 0.5f * gmn;
-                const float r = fmaxf(gmx - c, c - gmn);
-                int ex = 0;
-                if (r > 0.f && r <= 3.0e38f) {
-                    frexpf(r, &ex);  // r = f 2^ex, f in [0.5, 1)
-                    ex = 15 - ex;
-                    ex = ex < -120 ? -120 : (ex > 120 ? 120 : ex);
-                }
-                red[16] = (float)ex;
-                red[17] = (c == c && fabsf(c) <= 3.0e38f) ? c : 0.f;
-            }
-            __syncthreads();
-            const int ex = (int)red[16];
-            centre = red[17];
-            escale = ldexpf(1.f, ex);
-            unscale = a.tap_unscale * ldexpf(1.f, -ex);
+            tc_commit(drained);  // fires once every MMA issued above has completed
         }
-        const float offset = fmaf(centre, a.tap_sum, a.delta);
-        for (int it = tid; it < items; it += kTcThreads) {
-            const int q = it % nq, s = it / nq;
-            float v[8][4];
-            load_item<Tin>(a, gy_base + 8 * s, gx_base + 4 * q, v);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                unsigned hi[4], lo[4];
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const float x0 = (v[2 * p][c] - centre) * escale, x1 = (v[2 * p + 1][c] - centre) * escale;
-                    const __half2 h = __floats2half2_rn(x0, x1);
-                    hi[p] = h2_bits(h);
-                    if constexpr (FSRC) {
-                        const float2 hf = __half22float2(h);
-                        lo[p] = h2_bits(__floats2half2_rn(x0 - hf.x, x1 - hf.y));
-                    }
+        __syncwarp();
+    } else {
+        // ---- staging and read-out.  A wait that times out skips its
+        // read-out but never leaves the loop: the staging steps of float
+        // tiles hold barriers that every worker must reach.
+        int k = 0, ptx = 0, pty = 0;
+        TileScale pts{};
+        for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++k) {
+            const int b = k & 1;
+            const int tx0 = (t % a.tiles_x) * kTcM, ty0 = (t / a.tiles_x) * kTcRows;
+            const TileScale ts = stage_tile<Tin>(a, g, sm, b, red, tx0, ty0, tid);
+            fence_async_smem();
+            mbar_arrive(&full[b]);
+            if (k >= 1) {
+                const int pb = b ^ 1;
+                if (mbar_wait(&mma[pb], (unsigned)((k - 1) >> 1) & 1u, a.err, kErrTcWait)) {
+                    tc_fence_after();
+                    epilogue_tile<Tout>(a, tbase, pb, ptx, pty, pts, tid);
+                    tc_fence_before();
                 }
-                const int off = g.a_off(4 * q + c, 8 * s);
-                *reinterpret_cast<uint4*>(sm + g.offA + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                if constexpr (FSRC)
-                    *reinterpret_cast<uint4*>(sm + g.offA + g.bytesA + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+                mbar_arrive(&tfree[pb]);
+            }
+            ptx = tx0;
+            pty = ty0;
+            pts = ts;
+        }
+        if (k >= 1) {
+            const int pb = (k - 1) & 1;
+            if (mbar_wait(&mma[pb], (unsigned)((k - 1) >> 1) & 1u, a.err, kErrTcWait)) {
+                tc_fence_after();
+                epilogue_tile<Tout>(a, tbase, pb, ptx, pty, pts, tid);
+                tc_fence_before();
             }
         }
-        fence_async_smem();
-        __syncthreads();
-
-        // ---- 3. MMAs
-        if (tid == 0) {
-            tc_fence_after();
-            const uint32_t a0 = sm_base + g.offA, a1 = a0 + g.bytesA, b0 = sm_base, b1 = sm_base + g.bytesB;
-            for (int gi = 0; gi < kTcGroups; ++gi) {
-                const uint32_t dm = tbase + (uint32_t)(kTcN * gi), dc = dm + (uint32_t)kCorrCol;
-                uint32_t acc = 0;
-                for (int i = 0; i < a.kw; ++i) {
-                    const uint32_t ash = (uint32_t)(i + g.axa - a.ax) * 16u;
-                    for (int ks = 0; ks < g.Kt / 16; ++ks) {
-                        const uint32_t aoff = (uint32_t)(2 * gi + 2 * ks) * (uint32_t)g.lboA + ash;
-                        const uint32_t boff = (uint32_t)(i * g.bytesBi + 2 * ks * 256);
-                        const uint64_t da0 = tc_smem_desc(a0 + aoff, g.lboA, 128);
-                        const uint64_t db0 = tc_smem_desc(b0 + boff, 256, 128);
-                        const uint64_t db1 = tc_smem_desc(b1 + boff, 256, 128);
-                        tc_mma(dm, da0, db0, acc);
-                        tc_mma(dc, da0, db1, acc);
-                        if constexpr (FSRC) tc_mma(dc, tc_smem_desc(a1 + aoff, g.lboA, 128), db0, 1u);
-                        acc = 1u;
-                    }
-                }
-            }
-            tc_commit(bar);
-        }
-
-        // ---- 4. wait, read the accumulators, store
-        ok = mbar_wait(bar, phase, a.err, kErrTcWait);
-        ok = __syncthreads_and(ok) != 0;
-        if (!ok) break;
-        phase ^= 1u;
-        tc_fence_after();
-        const int m = 32 * (warp & 3) + lane;
-        const int x = tx0 + m;
-        const int c0 = (warp >> 2) * 32;  // first accumulator column of this warp
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            float v[16], w[16];
-            const uint32_t ta = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(c0 + 16 * h);
-            tmem_ld16(ta, v);
-            tmem_ld16(ta + (uint32_t)kCorrCol, w);
-            if (x < a.W) {
-#pragma unroll
-                for (int n = 0; n < 16; ++n) {
-                    const int y = ty0 + c0 + 16 * h + n;
-                    if (y < a.H)
-                        row_ptr_mut<Tout>(a.dst, a.dpitch, y)[x] = sat_from_f<Tout>(fmaf(v[n] + w[n], unscale, offset));
-                }
-            }
-        }
-        tc_fence_before();
-        __syncthreads();  // accumulators and the staged tile are free again
     }
 
-    // ---- teardown: no MMA may still run when the columns are freed
-    if (!ok && tid == 0) mbar_wait(bar, phase, a.err, kErrTcWait);
-    tc_fence_before();
+    // ---- teardown: every MMA has completed before the columns are freed
     __syncthreads();
-    tc_fence_after();
-    if (warp == 0)
+    if (warp == 0) {
+        if (lane == 0) mbar_wait(drained, 0, a.err, kErrTcWait);
+        __syncwarp();
+        tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
+    }
 }
 
 bool tc_supported(int sdt, int ddt) {
@@ -329,14 +436,19 @@ cudaError_t tc_launch_typed(const F2DTcArgs& a, const TcGeom& g, cudaStream_t s)
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     const int grid = a.ntiles < sms ? a.ntiles : sms;
-    if (g.alloc > 227 * 1024) return cudaErrorInvalidConfiguration;
-    filter2d_tc_kernel<Tin, Tout><<<grid, kTcThreads, g.alloc, s>>>(a);
+    if (g.smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+    // One CTA per SM: it allocates all 512 tensor-memory columns, so a second
+    // resident CTA would only wait for them.  Asking for more than half the
+    // SM's shared memory keeps the second one off.
+    const int smem = g.smem > 120 * 1024 ? g.smem : 120 * 1024;
+    filter2d_tc_kernel<Tin, Tout><<<grid, kTcThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-// Builds the two B parts (taps hi and lo, scaled by 2^s) in the shared layout.
+// Builds B (taps hi in rows 0-15, lo in rows 16-31, scaled by 2^s) in the
+// shared layout.
 void tc_build_b(const TcGeom& g, const float* taps, std::vector<__half>& out, float* tap_unscale) {
     double mx = 0;
     for (int j = 0; j < g.kh; ++j)
@@ -347,7 +459,7 @@ void tc_build_b(const TcGeom& g, const float* taps, std::vector<__half>& out, fl
         ex = 15 - ex;  // max |w| * 2^s in [2^14, 2^15)
     }
     *tap_unscale = (float)std::ldexp(1.0, -ex);
-    out.assign((size_t)g.bytesB, __float2half(0.f));  // 2 parts x bytesB / 2 halves
+    out.assign((size_t)g.bytesB / 2, __float2half(0.f));
     for (int i = 0; i < g.kw; ++i)
         for (int n = 0; n < kTcN; ++n)
             for (int j = 0; j < g.kh; ++j) {
@@ -355,9 +467,8 @@ void tc_build_b(const TcGeom& g, const float* taps, std::vector<__half>& out, fl
                 const double w = std::ldexp((double)taps[(size_t)j * g.kw + i], ex);
                 const __half hi = __double2half(w);
                 const __half lo = __double2half(w - (double)__half2float(hi));
-                const size_t o = (size_t)g.b_off(i, n, k) / 2;
-                out[o] = hi;
-                out[(size_t)g.bytesB / 2 + o] = lo;
+                out[(size_t)g.b_off(i, n, k) / 2] = hi;
+                out[(size_t)g.b_off(i, kTcN + n, k) / 2] = lo;
             }
 }
 

@@ -7,9 +7,10 @@
 // of 128 output pixels (x = tx0 + m) by NG x 16 output rows
 // (y = ty0 + 16 g + n), NG groups of MMAs
 //
-//   D_g[m][n] = sum_i sum_k A_{g,i}[m][k] * B_i[n][k]          (M=128, N=16)
+//   D_g[m][n] = sum_i sum_k A_{g,i}[m][k] * B_i[n][k]          (M=128, N=32)
 //   A_{g,i}[m][k] = T[m + sh_i][16 g + k],   sh_i = i + (axa - ax)
-//   B_i[n][k]     = w[k - n][i]  for 0 <= k - n < kh, else 0
+//   B_i[n][k]     = w_hi[k - n][i],  B_i[16 + n][k] = w_lo[k - n][i]
+//                   for 0 <= k - n < kh and n < 16, else 0
 //
 // where T[x'][r] = P[ty0 - ay + r][tx0 - axa + x'] is the source tile stored
 // transposed (x' major, source rows r contiguous) and axa = ax rounded up to
@@ -23,7 +24,10 @@
 // into hi = fp16(p * 2^e) and lo = fp16(p * 2^e - hi) with a per-tile power
 // of two 2^e; taps into hi = fp16(w * 2^s), lo = fp16(w * 2^s - hi).  The
 // products hi*hi + hi*lo + lo*hi (lo*lo dropped; uint8: A*hi + A*lo) are
-// accumulated in FP32 in tensor memory and scaled back by 2^-(e+s).  Pixels
+// accumulated in FP32 in tensor memory and scaled back by 2^-(e+s).  The hi
+// and lo taps sit side by side in B's N dimension, so one N = 32 MMA reads
+// the pixel tile once and fills both the hi x hi ("main", columns 0-15) and
+// the correction (columns 16-31) accumulator of its group.  Pixels
 // are centred first (uint8: p - 128, exact; float: about the tile's mid-range)
 // and hi*hi goes to its own accumulator, apart from the small correction
 // products, which keeps the accumulators small and their rounding low.
@@ -34,10 +38,11 @@
 namespace ipfc {
 
 constexpr int kTcM = 128;          // output pixels per tile (MMA M)
-constexpr int kTcN = 16;           // output rows per MMA group (MMA N)
+constexpr int kTcN = 16;           // output rows per MMA group (N = 2 x 16: hi and lo taps)
 constexpr int kTcGroups = 4;       // MMA groups per tile
 constexpr int kTcRows = kTcN * kTcGroups;
-constexpr int kTcThreads = 256;
+constexpr int kTcWorkers = 256;                // staging and epilogue threads (8 warps)
+constexpr int kTcThreads = kTcWorkers + 32;    // + the MMA-issuing warp
 constexpr int kTcMaxKw = 32;
 constexpr int kTcMaxKh = 33;
 
@@ -49,13 +54,12 @@ struct TcGeom {
     int KR;      // staged source rows (multiple of 8)
     int lboA;    // bytes between A's 8-row K slabs (= XR * 16)
     int bytesA;  // one A part
-    int bytesBi; // one tap column of one B part
-    int bytesB;  // one B part (kw columns)
+    int bytesBi; // B of one tap column (32 rows: hi, lo)
+    int bytesB;  // B of all kw tap columns
     int partsA;  // 1 (uint8) or 2 (float hi, lo)
     int offA;    // shared offsets
     int offBar;
-    int smem;   // bytes the layout uses
-    int alloc;  // bytes allocated (>= smem)
+    int smem;
 
     __host__ __device__ TcGeom(int kw_, int kh_, int ax_, int ay_, bool float_src) {
         kw = kw_;
@@ -68,27 +72,20 @@ struct TcGeom {
         KR = 16 * (kTcGroups - 1) + Kt;
         lboA = XR * 16;
         bytesA = (KR / 8) * lboA;
-        bytesBi = (Kt / 8) * 256;
+        bytesBi = (Kt / 8) * 512;
         bytesB = kw * bytesBi;
         partsA = float_src ? 2 : 1;
-        offA = 2 * bytesB;
-        offBar = offA + partsA * bytesA;
-        smem = offBar + 128;
-        // Allocation: also covers every address an A descriptor could reach
-        // with its two strides read the other way round (8-row groups LBO
-        // apart, K halves 128 bytes apart), so no operand read can leave the
-        // CTA's shared memory whatever the layout interpretation.
-        const int a_last = (partsA - 1) * bytesA + (2 * (kTcGroups - 1) + Kt / 8 - 2) * lboA +
-                           (kw - 1 + (axa - ax)) * 16;
-        const int swapped_end = offA + a_last + 15 * lboA + 7 * 16 + 128 + 16;
-        alloc = swapped_end > smem ? swapped_end : smem;
-        alloc = (alloc + 127) / 128 * 128;
+        offA = bytesB;                              // A: 2 buffers x partsA parts
+        offBar = offA + 2 * partsA * bytesA;
+        smem = offBar + 192;
     }
+    // shared offset of A buffer b, part p
+    __host__ __device__ int a_buf(int b, int p) const { return offA + (b * partsA + p) * bytesA; }
     // byte offset of T[x'][r] in an A part
     __host__ __device__ int a_off(int xr, int r) const { return (r >> 3) * lboA + xr * 16 + (r & 7) * 2; }
-    // byte offset of B_i[n][k] in a B part
+    // byte offset of B_i[n][k], n in [0, 32)
     __host__ __device__ int b_off(int i, int n, int k) const {
-        return i * bytesBi + (k >> 3) * 256 + (n >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2;
+        return i * bytesBi + (k >> 3) * 512 + (n >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2;
     }
 };
 
@@ -99,7 +96,9 @@ __host__ __device__ inline uint64_t tc_smem_desc(uint32_t addr, uint32_t lbo, ui
 }
 
 // Instruction descriptor of kind::f16: D f32, A and B f16, both K-major,
-// N = 16, M = 128.
-constexpr uint32_t kTcIdesc = (1u << 4) | ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+// M = 128, N = n.
+__host__ __device__ constexpr uint32_t tc_idesc(int n) {
+    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+}
 
 }  // namespace ipfc
