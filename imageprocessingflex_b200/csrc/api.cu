@@ -273,18 +273,24 @@ int deriv_taps(int order, int ksize, std::vector<double>& k) {
 // Separable path shared by sepFilter2D, gaussianBlur and sobel.
 // ---------------------------------------------------------------------------
 
-// Kernel selection for separable filters: IPFC_SEP_PATH=generic forces the
-// generic fused/two-pass kernels (used to check one form against the other).
 bool filter2d_tc_eligible(int sdt, int ddt, int C, int kw, int kh);
 cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spitch, void* dst, long long dpitch, int W,
                                int H, const float* taps, int kw, int kh, int ax, int ay, int border, float delta,
                                float bv, cudaStream_t s);
+bool sep_tc_launch(const void* src, long long spitch, void* dst, long long dpitch, int W, int H, int C,
+                   const double* kx, const double* ky, int K, int border, double delta, double bv, int clamp,
+                   cudaStream_t s, cudaError_t* err);
 
+// Kernel selection for separable filters.  Default: the CUDA-core fast
+// kernel where it is instantiated, else the generic kernels.
+// IPFC_SEP_PATH=generic forces the generic fused/two-pass kernels; =tc
+// selects the tensor-core column-pass kernel (sep_tc.cu) where it is
+// instantiated -- correct, but slower than the fast kernel on B200 so far.
 static int sep_path_mode() {
     static int mode = -1;
     if (mode < 0) {
         const char* v = std::getenv("IPFC_SEP_PATH");
-        mode = (v && std::strcmp(v, "generic") == 0) ? 1 : 0;
+        mode = (v && std::strcmp(v, "generic") == 0) ? 1 : (v && std::strcmp(v, "tc") == 0) ? 3 : 0;
     }
     return mode;
 }
@@ -374,6 +380,10 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
     if (!make_sep_fast_args(src, dst, in.ptr, in.pitch, out.ptr, out.pitch, kx, kw, ky, kh, ax, ay, border, delta, bv,
                             &f))
         return false;
+    if (sep_path_mode() == 3 && src->dtype == IPFC_U8 && dst->dtype == IPFC_U8 &&
+        sep_tc_launch(in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, kx, ky, kw, border,
+                      delta, bv, f.clamp, s, e))
+        return true;
     return sep_fast_dispatch(kw, src->channels, src->dtype, dst->dtype, f, s, e);
 }
 static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh, int ax,

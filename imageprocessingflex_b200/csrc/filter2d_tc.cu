@@ -32,7 +32,7 @@
 #include "../../include/ipfc.h"
 #include "common.cuh"
 #include "filter2d_tc.cuh"
-#include "tma.cuh"
+#include "tc_common.cuh"
 
 namespace ipfc {
 
@@ -59,38 +59,6 @@ struct F2DTcArgs {
 };
 
 namespace {
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                       uint32_t accumulate) {
-    const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
-}
-
-__device__ __forceinline__ void tc_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
 
 // Tensor memory: two accumulator sets (double buffer, 256 columns apart).
 // Group g of a set owns columns 64 g .. 64 g + 63: tap columns i of even
@@ -143,11 +111,6 @@ __device__ __forceinline__ void load_item(const F2DTcArgs& a, int gy0, int gx0, 
     }
 }
 
-__device__ __forceinline__ unsigned h2_bits(__half2 h) { return *reinterpret_cast<unsigned*>(&h); }
-
-// Barrier among the staging / epilogue warps only (the issuer warp is not
-// part of it).
-__device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kTcWorkers) : "memory"); }
 
 // Per-tile scaling of the staged operands and of the results.
 struct TileScale {
@@ -192,7 +155,7 @@ __device__ __forceinline__ TileScale stage_tile(const F2DTcArgs& a, const TcGeom
             red[warp] = mx;
             red[8 + warp] = mn;
         }
-        workers_sync();
+        workers_sync<kTcWorkers>();
         if (wtid == 0) {
             float gmx = -3.4e38f, gmn = 3.4e38f;
             for (int w = 0; w < kTcWorkers / 32; ++w) {
@@ -210,7 +173,7 @@ __device__ __forceinline__ TileScale stage_tile(const F2DTcArgs& a, const TcGeom
             red[16] = (float)ex;
             red[17] = (c == c && fabsf(c) <= 3.0e38f) ? c : 0.f;
         }
-        workers_sync();
+        workers_sync<kTcWorkers>();
         const int ex = (int)red[16];
         ts.centre = red[17];
         ts.escale = ldexpf(1.f, ex);

@@ -17,8 +17,10 @@
 //    outside the image;
 //  * compute: 4 adjacent samples per 32-bit word.  The row pass takes, for
 //    each window column i, the 4 bytes at staged offset 4t + i*C + delta
-//    (two aligned shared words and one byte permute) and folds them with a
-//    per-byte min/max; the column pass folds sh row-pass words;
+//    (two aligned shared words and one byte permute), spreads them over two
+//    words of 16-bit lanes (bytes 0, 2 and bytes 1, 3) and folds them with
+//    min/max.u16x2 (native; per-byte forms are emulated); the column pass
+//    folds sh row-pass word pairs and packs the bytes back once;
 //  * store: one 32-bit store per 4 outputs when the destination address is
 //    4-byte aligned, byte stores otherwise (rows of odd pitch).
 #pragma once
@@ -29,8 +31,21 @@ namespace ipfc {
 
 constexpr int kMorphU8Threads = 256;
 
-__device__ __forceinline__ unsigned bmin4(unsigned a, unsigned b) { return __vminu4(a, b); }
-__device__ __forceinline__ unsigned bmax4(unsigned a, unsigned b) { return __vmaxu4(a, b); }
+// 16-bit lane min / max (two lanes per instruction)
+__device__ __forceinline__ unsigned umin2(unsigned a, unsigned b) {
+    unsigned r;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned umax2(unsigned a, unsigned b) {
+    unsigned r;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+// bytes (b0, b1, b2, b3) -> lanes (b0, b2) and (b1, b3), and back
+__device__ __forceinline__ unsigned lanes_even(unsigned w) { return __byte_perm(w, 0u, 0x4240u); }
+__device__ __forceinline__ unsigned lanes_odd(unsigned w) { return __byte_perm(w, 0u, 0x4341u); }
+__device__ __forceinline__ unsigned lanes_pack(unsigned ev, unsigned od) { return __byte_perm(ev, od, 0x6240u); }
 
 // Bytes [s, s+4) of the staged row `w` (32-bit words), s >= 0.
 __device__ __forceinline__ unsigned staged_word(const unsigned* w, int s) {
@@ -49,9 +64,9 @@ struct MorphU8Geom {
         SP = ((SWB + 15 + 16) / 16) * 16 + 16;  // delta + samples + the last word's neighbour
         TW = TX / 4;
     }
-    // staged rows, row-pass rows, per-row offsets
+    // staged rows, row-pass rows (two words of 16-bit lanes per 4 samples), per-row offsets
     __host__ __device__ size_t bytes() const {
-        return (size_t)RY * SP + (size_t)RY * TW * 4 + (size_t)RY * 4;
+        return (size_t)RY * SP + (size_t)RY * TW * 8 + (size_t)RY * 4;
     }
 };
 
@@ -60,8 +75,8 @@ __host__ __device__ inline size_t morph_u8_tile_bytes(int TX, int TY, int sw, in
 }
 
 template <bool IS_MIN>
-__device__ __forceinline__ unsigned bfold(unsigned a, unsigned b) {
-    return IS_MIN ? bmin4(a, b) : bmax4(a, b);
+__device__ __forceinline__ unsigned fold2(unsigned a, unsigned b) {
+    return IS_MIN ? umin2(a, b) : umax2(a, b);
 }
 
 template <bool IS_MIN>
@@ -69,7 +84,7 @@ __device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, i
                                                    unsigned char* smem) {
     const MorphU8Geom g(TX, TY, a.sw, a.sh, a.C);
     unsigned char* stage = smem;
-    unsigned* hrow = reinterpret_cast<unsigned*>(smem + (size_t)g.RY * g.SP);
+    uint2* hrow = reinterpret_cast<uint2*>(smem + (size_t)g.RY * g.SP);
     int* delta = reinterpret_cast<int*>(hrow + (size_t)g.RY * g.TW);
     const int C = a.C;
     const int rowlen = a.W * C;
@@ -122,9 +137,14 @@ __device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, i
         const int r = it / g.TW, t = it - r * g.TW;
         const unsigned* w = reinterpret_cast<const unsigned*>(stage + (size_t)r * g.SP);
         const int s0 = 4 * t + delta[r];
-        unsigned acc = staged_word(w, s0);
-        for (int i = 1; i < a.sw; ++i) acc = bfold<IS_MIN>(acc, staged_word(w, s0 + i * C));
-        hrow[it] = acc;
+        const unsigned w0 = staged_word(w, s0);
+        unsigned ev = lanes_even(w0), od = lanes_odd(w0);
+        for (int i = 1; i < a.sw; ++i) {
+            const unsigned wi = staged_word(w, s0 + i * C);
+            ev = fold2<IS_MIN>(ev, lanes_even(wi));
+            od = fold2<IS_MIN>(od, lanes_odd(wi));
+        }
+        hrow[it] = make_uint2(ev, od);
     }
     __syncthreads();
 
@@ -133,8 +153,13 @@ __device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, i
         const int y = it / g.TW, t = it - y * g.TW;
         const int gy = y0 + y, q = q0 + 4 * t;
         if (gy >= a.H || q >= rowlen) continue;
-        unsigned acc = hrow[it];
-        for (int j = 1; j < a.sh; ++j) acc = bfold<IS_MIN>(acc, hrow[it + j * g.TW]);
+        uint2 h = hrow[it];
+        for (int j = 1; j < a.sh; ++j) {
+            const uint2 hj = hrow[it + j * g.TW];
+            h.x = fold2<IS_MIN>(h.x, hj.x);
+            h.y = fold2<IS_MIN>(h.y, hj.y);
+        }
+        const unsigned acc = lanes_pack(h.x, h.y);
         unsigned char* drow = reinterpret_cast<unsigned char*>(a.dst) + (long long)gy * a.dpitch;
         if (q + 4 <= rowlen && (((uintptr_t)(drow + q)) & 3) == 0) {
             *reinterpret_cast<unsigned*>(drow + q) = acc;
