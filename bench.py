@@ -727,25 +727,64 @@ def run_filter2d(args):
     return 0
 
 
-def launches_only(n):
-    """n plain launches of the workload on one resident image, no timing:
-    the program profiled by the ncu captures summarised under profiles/."""
+def launches_only(n, workload="headline"):
+    """n plain launches of a workload's main kernel on resident data, no
+    timing: the programs profiled by the ncu captures summarised under
+    profiles/.
+      headline -- gaussianBlur(sigma=2) on one 3840x2160x3 uint8 image;
+      filter2d -- the split-precision tcgen05 filter2D, 31x31 seeded N(0,1)
+                  taps, on one 4096x4096 uint8 image;
+      batch    -- the 512-image uneven mix as one batch (plan, then n runs)."""
     import torch
 
     import imageprocessingflex_b200 as ipf
 
-    x = torch.from_numpy(seeded_image(W_IMG, H_IMG, C_IMG)).cuda()
-    for _ in range(n):
-        y = ipf.gaussianBlur(x, SIGMA)
+    if workload == "filter2d":
+        from imageprocessingflex_b200 import mix
+
+        g = torch.Generator(device="cuda")
+        g.manual_seed(3)
+        x = torch.randint(0, 256, (4096, 4096), generator=g, device="cuda", dtype=torch.int32).to(torch.uint8)
+        taps = mix.filter2d_taps(31, seed=1031)
+        for _ in range(n):
+            y = ipf.filter2D(x, taps, form="split")
+    elif workload == "batch":
+        from imageprocessingflex_b200 import batch as B
+        from imageprocessingflex_b200 import mix
+
+        items = mix.uneven_mix(512, seed=2024)
+        b = B.Batch()
+        keep = []
+        for it in items:
+            shape = (it.height, it.width, it.channels) if it.channels > 1 else (it.height, it.width)
+            s_ = torch.empty(shape, dtype=torch.uint8, device="cuda")
+            mix.fill_uniform_u8(s_, it.seed)
+            d_ = torch.empty_like(s_)
+            keep += [s_, d_]
+            if it.op == "gaussian":
+                b.add_gaussianBlur(s_, d_, it.sigma)
+            elif it.op == "median":
+                b.add_medianBlur(s_, d_, it.ksize)
+            elif it.op == "erode":
+                b.add_erode(s_, d_)
+            else:
+                b.add_dilate(s_, d_)
+        for _ in range(n):
+            b.run()
+        y = keep[-1]
+    else:
+        x = torch.from_numpy(seeded_image(W_IMG, H_IMG, C_IMG)).cuda()
+        for _ in range(n):
+            y = ipf.gaussianBlur(x, SIGMA)
     torch.cuda.synchronize()
-    print(f"{n} launches done, checksum {int(y.sum().item())}")
+    print(f"{n} launches done ({workload}), checksum {int(y.to(torch.int64).sum().item())}")
     return 0
 
 
 def main():
     args = parse_args()
     if args.launches_only > 0:
-        return launches_only(args.launches_only)
+        return launches_only(args.launches_only, args.workload)
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "batch":
