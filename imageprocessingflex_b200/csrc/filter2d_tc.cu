@@ -7,10 +7,11 @@
 //     layout) is copied from global memory, 256 tensor-memory columns are
 //     allocated (two accumulator sets) and the barriers initialised;
 //  2. per tile, the workers stage the transposed source tile into one of two
-//     A buffers: 8 source rows x 4 pixels per work item, borders resolved at
-//     load, pixels centred and converted to FP16 (uint8: exact; float: hi
-//     and lo parts under a per-tile power of two), stored as 16-byte rows of
-//     K-major core matrices;
+//     A buffers, one tile ahead (loads issued before the previous tile's
+//     read-out): 8 source rows x 4 pixels per work item, borders resolved at
+//     load, pixels centred and converted to FP16 (uint8: exact, by byte
+//     permutes; float: hi and lo parts under a per-tile power of two),
+//     stored as 16-byte rows of K-major core matrices;
 //  3. one thread of the MMA warp issues the tile's MMAs -- 4 groups x kw tap
 //     columns x Kt/16 K steps, each one N = 32 MMA (hi and lo taps) plus,
 //     for float sources, one N = 16 MMA (lo pixels x hi taps) -- into one of
@@ -54,6 +55,8 @@ struct F2DTcArgs {
     float tap_unscale;  // 2^-s
     float tap_sum;      // sum of the taps (FP64 on the host, rounded once)
     int tiles_x, ntiles;
+    int byte_border;    // uint8 source whose Constant border value (if any) is a byte: packed staging
+    unsigned char bvb;  // that byte
     const uint4* btab;  // B in the shared layout
     unsigned* err;
 };
@@ -119,6 +122,127 @@ struct TileScale {
     float unscale;  // 2^-(e+s): accumulator -> result
     float offset;   // centre * sum(taps) + delta
 };
+
+constexpr int kTcItemsPerThread = 2;  // staging items per worker (XR/4 x KR/8 <= 42 x 12 <= 512)
+
+// uint8 source, prefetch form: 8 rows x 4 pixels at (gy0, gx0) as one word
+// (4 bytes) per row, borders resolved, Constant as the border byte.
+__device__ __forceinline__ void load_item_raw(const F2DTcArgs& a, int gy0, int gx0, unsigned (&w)[8]) {
+    const bool cols_in = gx0 >= 0 && gx0 + 4 <= a.W;
+    int cx[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) cx[c] = cols_in ? gx0 + c : border_index(gx0 + c, a.W, a.border);
+    const unsigned cfill = 0x01010101u * a.bvb;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int sy = border_index(gy0 + j, a.H, a.border);
+        if (sy < 0) {
+            w[j] = cfill;
+            continue;
+        }
+        const uint8_t* row = row_ptr<uint8_t>(a.src, a.spitch, sy);
+        if (cols_in && (((uintptr_t)(row + gx0)) & 3) == 0) {
+            w[j] = __ldg(reinterpret_cast<const unsigned*>(row + gx0));
+            continue;
+        }
+        unsigned x = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) x |= (cx[c] < 0 ? (unsigned)a.bvb : (unsigned)__ldg(row + cx[c])) << (8 * c);
+        w[j] = x;
+    }
+}
+
+// Stores one prefetched uint8 item: pixel c's 8 rows as FP16 (b - 128),
+// exact -- byte b -> f16 bits 0x6400 | b (= 1024 + b) by byte permutes, minus
+// 1152 (0x6480).  Lanes store their four 16-byte rows in rotated order, so
+// one store instruction's rows land 80 bytes apart, on distinct bank groups.
+__device__ __forceinline__ void store_item_raw(unsigned char* A, const TcGeom& g, int q, int s, const unsigned (&w)[8],
+                                               int rot) {
+    const __half2 k1152 = __halves2half2(__ushort_as_half((unsigned short)0x6480), __ushort_as_half((unsigned short)0x6480));
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) {
+        const unsigned c = (unsigned)((cc + rot) & 3);
+        const unsigned sel = c | ((4u + c) << 4);
+        unsigned h[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const unsigned t = __byte_perm(w[2 * p], w[2 * p + 1], sel);
+            const unsigned u = __byte_perm(t, 0x64646464u, 0x4140u);
+            const __half2 v = __hsub2(*reinterpret_cast<const __half2*>(&u), k1152);
+            h[p] = h2_bits(v);
+        }
+        *reinterpret_cast<uint4*>(A + g.a_off(4 * q + (int)c, 8 * s)) = make_uint4(h[0], h[1], h[2], h[3]);
+    }
+}
+
+// Per-tile centre and power of two of a float tile from each worker's local
+// max / min (all worker threads): max |p - centre| * 2^e in [2^14, 2^15).
+__device__ __forceinline__ TileScale tile_scale_from(const F2DTcArgs& a, float* red, float mx, float mn, int wtid) {
+    const int warp = wtid >> 5, lane = wtid & 31;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    if (lane == 0) {
+        red[warp] = mx;
+        red[8 + warp] = mn;
+    }
+    workers_sync<kTcWorkers>();
+    if (wtid == 0) {
+        float gmx = -3.4e38f, gmn = 3.4e38f;
+        for (int w = 0; w < kTcWorkers / 32; ++w) {
+            gmx = fmaxf(gmx, red[w]);
+            gmn = fminf(gmn, red[8 + w]);
+        }
+        const float c = 0.5f * gmx + 0.5f * gmn;
+        const float r = fmaxf(gmx - c, c - gmn);
+        int ex = 0;
+        if (r > 0.f && r <= 3.0e38f) {
+            frexpf(r, &ex);  // r = f 2^ex, f in [0.5, 1)
+            ex = 15 - ex;
+            ex = ex < -120 ? -120 : (ex > 120 ? 120 : ex);
+        }
+        red[16] = (float)ex;
+        red[17] = (c == c && fabsf(c) <= 3.0e38f) ? c : 0.f;
+    }
+    workers_sync<kTcWorkers>();
+    const int ex = (int)red[16];
+    TileScale ts;
+    ts.centre = red[17];
+    ts.escale = ldexpf(1.f, ex);
+    ts.unscale = a.tap_unscale * ldexpf(1.f, -ex);
+    ts.offset = fmaf(ts.centre, a.tap_sum, a.delta);
+    return ts;
+}
+
+// Stores one prefetched float item as FP16 hi and lo parts of the centred,
+// scaled pixels (rotated chunk order, as store_item_raw).
+__device__ __forceinline__ void store_item_split(unsigned char* A0, unsigned char* A1, const TcGeom& g, int q, int s,
+                                                 const float (&v)[8][4], const TileScale& ts, int rot) {
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) {
+        const int c = (cc + rot) & 3;
+        unsigned hi[4], lo[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            float x0 = 0.f, x1 = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k == c) {
+                    x0 = (v[2 * p][k] - ts.centre) * ts.escale;
+                    x1 = (v[2 * p + 1][k] - ts.centre) * ts.escale;
+                }
+            const __half2 h = __floats2half2_rn(x0, x1);
+            hi[p] = h2_bits(h);
+            const float2 hf = __half22float2(h);
+            lo[p] = h2_bits(__floats2half2_rn(x0 - hf.x, x1 - hf.y));
+        }
+        const int off = g.a_off(4 * q + c, 8 * s);
+        *reinterpret_cast<uint4*>(A0 + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(A1 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    }
+}
 
 // Stages tile (tx0, ty0) into A buffer `abuf` (all worker threads).
 template <typename Tin>
@@ -341,38 +465,99 @@ __global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid
         }
         __syncwarp();
     } else {
-        // ---- staging and read-out.  A wait that times out skips its
-        // read-out but never leaves the loop: the staging steps of float
-        // tiles hold barriers that every worker must reach.
-        int k = 0, ptx = 0, pty = 0;
-        TileScale pts{};
-        for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++k) {
-            const int b = k & 1;
-            const int tx0 = (t % a.tiles_x) * kTcM, ty0 = (t / a.tiles_x) * kTcRows;
-            const TileScale ts = stage_tile<Tin>(a, g, sm, b, red, tx0, ty0, tid);
+        // ---- staging and read-out.  This CTA's tiles are t_j = blockIdx.x +
+        // j gridDim.x.  Tile j+1 is staged one step ahead: in step j the
+        // workers issue tile j+1's loads, read tile j-1 out while the tensor
+        // cores run tile j, then convert and store tile j+1 (A buffer (j+1)
+        // mod 2, free since tile j-1's MMAs completed).  A wait that times out
+        // skips its read-out but never leaves the loop: the staging steps of
+        // float tiles hold barriers that every worker must reach.
+        const int nq = g.XR / 4, ns = g.KR / 8, items = nq * ns;
+        const int ntl = a.ntiles > (int)blockIdx.x ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+        const bool packed = !FSRC && a.byte_border;
+        TileScale sc0{}, sc1{};  // scales of the tiles in A buffers 0 and 1
+        auto tile_xy = [&](int j, int& tx0, int& ty0) {
+            const int t = (int)blockIdx.x + j * (int)gridDim.x;
+            tx0 = (t % a.tiles_x) * kTcM;
+            ty0 = (t / a.tiles_x) * kTcRows;
+        };
+        unsigned raw[kTcItemsPerThread][8];
+        float fv[FSRC ? kTcItemsPerThread : 1][8][4];
+        auto issue_loads = [&](int j) {
+            int tx0, ty0;
+            tile_xy(j, tx0, ty0);
+#pragma unroll
+            for (int r = 0; r < kTcItemsPerThread; ++r) {
+                const int it = tid + r * kTcWorkers;
+                if (it >= items) continue;
+                const int gy0 = ty0 - a.ay + 8 * (it / nq), gx0 = tx0 - g.axa + 4 * (it % nq);
+                if constexpr (FSRC) load_item<Tin>(a, gy0, gx0, fv[r]);
+                else if (packed) load_item_raw(a, gy0, gx0, raw[r]);
+            }
+        };
+        auto store_tile = [&](int j) {
+            int tx0, ty0;
+            tile_xy(j, tx0, ty0);
+            const int b = j & 1;
+            if constexpr (FSRC) {
+                float mx = -3.4e38f, mn = 3.4e38f;
+#pragma unroll
+                for (int r = 0; r < kTcItemsPerThread; ++r) {
+                    if (tid + r * kTcWorkers >= items) continue;
+#pragma unroll
+                    for (int jj = 0; jj < 8; ++jj)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            mx = fmaxf(mx, fv[r][jj][c]);
+                            mn = fminf(mn, fv[r][jj][c]);
+                        }
+                }
+                const TileScale ts = tile_scale_from(a, red, mx, mn, tid);
+                unsigned char* A0 = sm + g.a_buf(b, 0);
+                unsigned char* A1 = sm + g.a_buf(b, 1);
+#pragma unroll
+                for (int r = 0; r < kTcItemsPerThread; ++r) {
+                    const int it = tid + r * kTcWorkers;
+                    if (it < items) store_item_split(A0, A1, g, it % nq, it / nq, fv[r], ts, lane);
+                }
+                (b ? sc1 : sc0) = ts;
+            } else if (packed) {
+                unsigned char* A0 = sm + g.a_buf(b, 0);
+#pragma unroll
+                for (int r = 0; r < kTcItemsPerThread; ++r) {
+                    const int it = tid + r * kTcWorkers;
+                    if (it < items) store_item_raw(A0, g, it % nq, it / nq, raw[r], lane);
+                }
+                (b ? sc1 : sc0) = TileScale{1.f, 128.f, a.tap_unscale, fmaf(128.f, a.tap_sum, a.delta)};
+            } else {
+                (b ? sc1 : sc0) = stage_tile<Tin>(a, g, sm, b, red, tx0, ty0, tid);
+            }
             fence_async_smem();
             mbar_arrive(&full[b]);
-            if (k >= 1) {
-                const int pb = b ^ 1;
-                if (mbar_wait(&mma[pb], (unsigned)((k - 1) >> 1) & 1u, a.err, kErrTcWait)) {
-                    tc_fence_after();
-                    epilogue_tile<Tout>(a, tbase, pb, ptx, pty, pts, tid);
-                    tc_fence_before();
-                }
-                mbar_arrive(&tfree[pb]);
-            }
-            ptx = tx0;
-            pty = ty0;
-            pts = ts;
-        }
-        if (k >= 1) {
-            const int pb = (k - 1) & 1;
-            if (mbar_wait(&mma[pb], (unsigned)((k - 1) >> 1) & 1u, a.err, kErrTcWait)) {
+        };
+        auto read_out = [&](int j) {
+            const int pb = j & 1;
+            int px, py;
+            tile_xy(j, px, py);
+            if (mbar_wait(&mma[pb], (unsigned)(j >> 1) & 1u, a.err, kErrTcWait)) {
                 tc_fence_after();
-                epilogue_tile<Tout>(a, tbase, pb, ptx, pty, pts, tid);
+                epilogue_tile<Tout>(a, tbase, pb, px, py, pb ? sc1 : sc0, tid);
                 tc_fence_before();
             }
+        };
+        if (ntl > 0) {
+            issue_loads(0);
+            store_tile(0);
         }
+        for (int j = 0; j < ntl; ++j) {
+            if (j + 1 < ntl) issue_loads(j + 1);
+            if (j >= 1) {
+                read_out(j - 1);
+                mbar_arrive(&tfree[(j - 1) & 1]);
+            }
+            if (j + 1 < ntl) store_tile(j + 1);
+        }
+        if (ntl > 0) read_out(ntl - 1);
     }
 
     // ---- teardown: every MMA has completed before the columns are freed
@@ -472,6 +657,9 @@ cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spit
         a.tiles_x = (W + kTcM - 1) / kTcM;
         a.ntiles = a.tiles_x * ((H + kTcRows - 1) / kTcRows);
         a.btab = dbt;
+        a.byte_border = (sdt == IPFC_U8 && (border != IPFC_BORDER_CONSTANT ||
+                                            (bv >= 0.f && bv <= 255.f && bv == std::floor(bv)))) ? 1 : 0;
+        a.bvb = (border == IPFC_BORDER_CONSTANT && a.byte_border) ? (unsigned char)bv : 0;
         a.err = device_error_word();
         if (sdt == IPFC_F32) e = tc_launch_typed<float, float>(a, g, s);
         else if (ddt == IPFC_U8) e = tc_launch_typed<uint8_t, uint8_t>(a, g, s);
