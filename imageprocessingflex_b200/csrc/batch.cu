@@ -121,8 +121,9 @@ Tiling tile_item(BatchItem& it, int W, int H, TuneVal v) {
         t.nx = (W * it.C + it.tx - 1) / it.tx;
         t.ny = (H + it.ty - 1) / it.ty;
         if (it.kind == kBatchMedian) {
-            t.smem = median_tile_bytes(it.tx, it.ty, it.K, it.C);
-            t.cost = (double)it.tx * it.ty * it.K * it.K * 4;
+            t.smem = (it.K == 3 || it.K == 5) ? median_u8_tile_bytes(it.tx, it.ty, it.K, it.C)
+                                              : median_tile_bytes(it.tx, it.ty, it.K, it.C);
+            t.cost = (double)it.tx * it.ty * it.K * it.K * ((it.K == 3 || it.K == 5) ? 1 : 4);
         } else {
             const MorphCore& m = it.u.morph;
             t.smem = morph_u8_tile_bytes(it.tx, it.ty, m.sw, m.sh, it.C);
@@ -315,7 +316,8 @@ cudaError_t tune_key(const TuneKey& key, const HostItem& proto, TuneVal* best) {
         if (e != cudaSuccess) break;
         if (key.kind != kBatchSep) {
             const size_t need = key.kind == kBatchMedian
-                                    ? median_tile_bytes(v.a, v.b, key.k, C)
+                                    ? ((key.k == 3 || key.k == 5) ? median_u8_tile_bytes(v.a, v.b, key.k, C)
+                                                                  : median_tile_bytes(v.a, v.b, key.k, C))
                                     : morph_u8_tile_bytes(v.a, v.b, proto.it.u.morph.sw, proto.it.u.morph.sh, C);
             if (need > 96 * 1024) continue;
         }

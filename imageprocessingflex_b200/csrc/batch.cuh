@@ -9,7 +9,7 @@
 // expensive tiles come first.  Each CTA of the persistent kernel then loops:
 // take the next tile index from a global counter, copy the tile's item into
 // shared memory when it changes, and run the tile body (sep_fast_tile,
-// median_tile, morph_u8_tile).  The tile bodies are the per-image kernels'
+// median_u8_tile / median_tile, morph_u8_tile).  The tile bodies are the per-image kernels'
 // own code, so a batched image is computed exactly as the per-image call
 // computes it.
 //
@@ -21,6 +21,7 @@
 #pragma once
 
 #include "median.cuh"
+#include "median_u8.cuh"
 #include "morph.cuh"
 #include "morph_u8.cuh"
 #include "sep_fast.cuh"

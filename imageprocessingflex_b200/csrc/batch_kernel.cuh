@@ -21,7 +21,11 @@ __device__ __noinline__ void batch_sep_tile(int x, int y) {
 }
 
 static __device__ __noinline__ void batch_median_tile(int x, int y) {
-    median_tile<uint8_t>(g_batch_item.u.med, g_batch_item.tx, g_batch_item.ty, x, y, g_batch_smem);
+    if (g_batch_item.K == 3 || g_batch_item.K == 5)
+        median_u8_tile(g_batch_item.u.med, g_batch_item.tx, g_batch_item.ty, x, y,
+                       reinterpret_cast<unsigned char*>(g_batch_smem));
+    else
+        median_tile<uint8_t>(g_batch_item.u.med, g_batch_item.tx, g_batch_item.ty, x, y, g_batch_smem);
 }
 
 static __device__ __noinline__ void batch_morph_tile(int x, int y) {
