@@ -451,6 +451,15 @@ def run_batch(args):
         plain_step()
     ms_plain_graph = timed(g.replay, max(1, min(args.steps, 5)))
     del g
+    # where the per-image form's time goes: each op's images alone
+    by_op = {}
+    all_items, all_views = items, views
+    for op in ("gaussian", "median", "erode", "dilate"):
+        sel = [i for i, it in enumerate(all_items) if it.op == op]
+        items = [all_items[i] for i in sel]
+        views = [all_views[i] for i in sel]
+        by_op[op] = round(timed(plain_step, max(1, min(args.steps, 3))), 3)
+    items, views = all_items, all_views
 
     mpix = sum(it.pixels for it in items) / 1e6
     alg_bytes = 2.0 * sum(it.pixels * it.channels for it in items)
@@ -475,6 +484,7 @@ def run_batch(args):
         "plain": {"ms": round(ms_plain, 4), "mpix_s": round(mpix / (ms_plain / 1e3), 1),
                   "launches_per_step": len(items), "form": "one C-ABI call per image from the host"},
         "plain_graph": {"ms": round(ms_plain_graph, 4), "mpix_s": round(mpix / (ms_plain_graph / 1e3), 1)},
+        "plain_ms_by_op": by_op,
         "speedup_vs_plain": round(ms_plain / ms_batched, 3),
         "speedup_vs_plain_graph": round(ms_plain_graph / ms_batched, 3),
         "results_equal_per_image": same,
