@@ -93,7 +93,9 @@ struct FastGeom {
     static constexpr int VWP = VW4 + ((4 - VW4 % 32) + 32) % 32;
     static constexpr int PLANE = TB * VWP;
     static constexpr size_t PLANES_BYTES = sizeof(float) * (size_t)C * PLANE;
-    static constexpr size_t SMEM = PLANES_BYTES;
+    // border lanes' extra words: K rows x 2 words x one per thread
+    static constexpr size_t RING_BYTES = sizeof(unsigned) * 2 * K * kFastThreads;
+    static constexpr size_t SMEM = PLANES_BYTES + RING_BYTES;
 };
 
 // ---- packed FP32 (fma/add .f32x2, sm_100a) ----------------------------------
@@ -148,11 +150,13 @@ __device__ __forceinline__ int round_s_sat(float v, int lo, int hi) {
 }
 
 // Border rows: kept out of line so the in-range test is all the hot loop
-// executes for interior rows.
-static __device__ __noinline__ int border_row_slow(int y, int n, int mode) { return border_index(y, n, mode); }
-
-__device__ __forceinline__ int row_source(int y, int n, int mode) {
-    return ((unsigned)y < (unsigned)n) ? y : border_row_slow(y, n, mode);
+// executes for interior rows.  A row that reads the Constant value maps to
+// row 0 (any readable row: the caller replaces those samples).
+static __device__ __noinline__ int border_row_any_slow(int y, int n, int mode) {
+    return max(border_index(y, n, mode), 0);
+}
+__device__ __forceinline__ int row_any(int y, int n, int mode) {
+    return ((unsigned)y < (unsigned)n) ? y : border_row_any_slow(y, n, mode);
 }
 
 // Compile-time loop: f(std::integral_constant<int, I>) for I in [I0, N).
@@ -162,6 +166,19 @@ __device__ __forceinline__ void static_for(F&& f) {
         f(std::integral_constant<int, I>{});
         static_for<I + 1, N>(f);
     }
+}
+
+// 4-byte asynchronous copy global -> shared; only the first `n` (0..4) bytes
+// are read, the rest of the destination word is zero-filled.  The source is
+// 4-byte aligned.
+__device__ __forceinline__ void cp_async4(unsigned* dst, const void* src, int n) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // PRMT selector that replaces byte `pos` of the first operand with byte 0 of
@@ -282,7 +299,9 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
     const int g0 = (x0 - G::RX) * C;               // global sample of strip sample 0
     const int lead = g0 & (G::ALIGN - 1);          // thread groups start on an aligned global sample
     const int s0 = NCOL * tid - lead;
-    const bool active = s0 + NCOL - 1 >= 0 && s0 < G::IW;
+    // samples that a stored output reads: the strip's outputs inside the image and their halo
+    const int used = min(G::IW, (min(G::PX, a.W - x0) + G::HX) * C);
+    const bool active = s0 + NCOL - 1 >= 0 && s0 < used;
     int idx[NCOL];
     bool vec = active && a.vec_load;
 #pragma unroll
@@ -294,7 +313,82 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
     vec = vec && idx[0] >= 0 && (idx[0] & (NCOL - 1)) == 0;
     unsigned cmask = 0;  // columns that read the Constant border value
 #pragma unroll
-    for (int k = 0; k < NCOL; ++k) cmask |= (idx[k] < 0 ? 1u : 0u) << k;
+    for (int k = 0; k < NCOL; ++k) cmask |= (active && idx[k] < 0 ? 1u : 0u) << k;
+
+    // Load plan.  The row loop prefetches K rows ahead, and a prefetch only
+    // overlaps the work in between when it is one load straight into its ring
+    // register, the same instruction in every lane (a load whose value merges
+    // across a branch makes the warp wait for it).  So:
+    //  * every lane loads one aligned in-row word per row (element c0) into the
+    //    register ring: its own NCOL samples when they are in order and
+    //    aligned, any in-row word otherwise;
+    //  * a lane whose samples are border-mapped or straddle the row end also
+    //    copies the other aligned words that hold them (c1, c2; n1, n2 of their
+    //    bytes lie in the row, the rest is zero-filled and never read) into a
+    //    shared ring with cp.async, and assembles its samples at use -- two
+    //    byte permutes (8-bit) or a select (float).  Warps without such lanes
+    //    skip the copies (a warp-uniform branch, no register involved);
+    //  * unaligned sources (or a lane needing more than three words) fall back
+    //    to one load per sample for the warp.
+    // Lanes whose sample reads the Constant value take any byte there.
+    int c0 = 0, c1 = 0, c2 = 0, n1 = 0, n2 = 0;
+    unsigned selA = 0x3210u, selB = 0x3210u;  // 8-bit: t = prmt(reg, w1, selA); raw = prmt(t, w2, selB)
+    bool extra = false, fail = !a.vec_load || rowlen < NCOL;
+    if (!fail && active) {
+        if (vec) {
+            c0 = idx[0];
+        } else if constexpr (sizeof(Tin) == 1) {
+            int wk[NCOL];
+#pragma unroll
+            for (int k = 0; k < NCOL; ++k) wk[k] = idx[k] >= 0 ? (idx[k] & ~3) : -1;
+            // register word: the first word that lies wholly in the row (else word 0, unused)
+            int wa = -1;
+#pragma unroll
+            for (int k = NCOL - 1; k >= 0; --k)
+                if (wk[k] >= 0 && wk[k] + 4 <= rowlen) wa = wk[k];
+            c0 = wa < 0 ? 0 : wa;
+            int wb = -1, wc = -1;
+#pragma unroll
+            for (int k = 0; k < NCOL; ++k) {
+                const int w = wk[k];
+                if (w < 0 || w == wa || w == wb || w == wc) continue;
+                if (wb < 0) wb = w;
+                else if (wc < 0) wc = w;
+                else fail = true;
+            }
+            selA = 0;
+            selB = 0;
+#pragma unroll
+            for (int k = 0; k < NCOL; ++k) {
+                const int w = wk[k], p = idx[k] & 3;
+                const unsigned na = (w >= 0 && w == wb) ? 4u + p : (w >= 0 && w == wa) ? (unsigned)p : 0u;
+                const unsigned nb = (w >= 0 && w == wc && w != wa && w != wb) ? 4u + p : (unsigned)k;
+                selA |= na << (4 * k);
+                selB |= nb << (4 * k);
+            }
+            if (wb >= 0) {
+                c1 = wb;
+                n1 = min(4, rowlen - wb);
+            }
+            if (wc >= 0) {
+                c2 = wc;
+                n2 = min(4, rowlen - wc);
+            }
+            extra = selA != 0x3210u || selB != 0x3210u;
+        } else {
+            // float: each sample is its own word, both from the shared ring
+            extra = true;
+            c1 = max(idx[0], 0);
+            n1 = idx[0] >= 0 ? 4 : 0;
+            c2 = max(idx[1], 0);
+            n2 = idx[1] >= 0 ? 4 : 0;
+        }
+    }
+    const bool wbytes = __any_sync(0xffffffffu, fail);
+    const bool wextra = !wbytes && __any_sync(0xffffffffu, extra);
+#pragma unroll
+    for (int k = 0; k < NCOL; ++k) idx[k] = max(idx[k], 0);
+    unsigned* xring = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(vbuf) + G::PLANES_BYTES) + tid;
     int vdst[NCOL];  // shared offset of this column in band row 0 (-1: not stored)
 #pragma unroll
     for (int k = 0; k < NCOL; ++k) {
@@ -317,35 +411,38 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
     // The raw samples of the next K rows, loaded K rows ahead of use.
     using Raw = typename std::conditional<sizeof(Tin) == 1, unsigned, uint2>::type;
     Raw raw[K];
-    auto fetch = [&](int t) -> Raw {
+    // Rows past the last one walked are not loaded (a CTA-uniform test); rows
+    // outside the image resolve out of line, Constant rows to row 0 (their
+    // samples are replaced by the border value below).  `slot` is the ring
+    // position (t mod K), a compile-time constant at every call.
+    auto fetch = [&](int t, int slot) -> Raw {
         Raw r{};
-        if (t < T && active) {
-            const int sy = row_source(ybase + t, a.H, a.border);
-            if (sy >= 0) {
-                const Tin* srow = row_ptr<Tin>(a.src, a.spitch, sy);
+        if (t < T) {
+            const Tin* srow = row_ptr<Tin>(a.src, a.spitch, row_any(ybase + t, a.H, a.border));
+            if (!wbytes) {
                 if constexpr (sizeof(Tin) == 1) {
-                    if (vec) {
-                        r = __ldg(reinterpret_cast<const unsigned*>(srow + idx[0]));
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < NCOL; ++k)
-                            if (idx[k] >= 0) r |= (unsigned)__ldg(srow + idx[k]) << (8 * k);
-                    }
+                    r = __ldg(reinterpret_cast<const unsigned*>(srow + c0));
                 } else {
-                    if (vec) {
-                        const float2 v = __ldg(reinterpret_cast<const float2*>(srow + idx[0]));
-                        r = make_uint2(__float_as_uint(v.x), __float_as_uint(v.y));
-                    } else {
-                        if (idx[0] >= 0) r.x = __float_as_uint(static_cast<float>(__ldg(srow + idx[0])));
-                        if (idx[1] >= 0) r.y = __float_as_uint(static_cast<float>(__ldg(srow + idx[1])));
-                    }
+                    const float2 v = __ldg(reinterpret_cast<const float2*>(srow + c0));
+                    r = make_uint2(__float_as_uint(v.x), __float_as_uint(v.y));
                 }
+                if (wextra) {
+                    cp_async4(xring + (2 * slot) * kFastThreads, srow + c1, n1);
+                    cp_async4(xring + (2 * slot + 1) * kFastThreads, srow + c2, n2);
+                }
+            } else if constexpr (sizeof(Tin) == 1) {
+#pragma unroll
+                for (int k = 0; k < NCOL; ++k) r |= (unsigned)__ldg(srow + idx[k]) << (8 * k);
+            } else {
+                r = make_uint2(__float_as_uint(__ldg(srow + idx[0])), __float_as_uint(__ldg(srow + idx[1])));
             }
         }
+        if (wextra) cp_async_commit();
         return r;
     };
-    static_for<0, K>([&](auto U) { raw[decltype(U)::value] = fetch(decltype(U)::value); });
+    static_for<0, K>([&](auto U) { raw[decltype(U)::value] = fetch(decltype(U)::value, decltype(U)::value); });
     const f2p mbias = pk2(-8388608.0f, -8388608.0f);
+    const bool cfix = a.border == IPFC_BORDER_CONSTANT;  // Constant rows / columns take the border value
 
     for (int tb = 0; tb < T; tb += K) {
         static_for<0, K>([&](auto U) {
@@ -353,20 +450,27 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
             const int t = tb + u;
             if (t < T) {
                 f2p x[NP];
+                Raw v = raw[u];
+                if (wextra) {  // this row's copies: the oldest of the K groups in flight
+                    cp_async_wait<K - 1>();
+                    const unsigned w1 = xring[(2 * u) * kFastThreads], w2 = xring[(2 * u + 1) * kFastThreads];
+                    if constexpr (sizeof(Tin) == 1) v = __byte_perm(__byte_perm(v, w1, selA), w2, selB);
+                    else if (extra) v = make_uint2(w1, w2);
+                }
                 if constexpr (sizeof(Tin) == 1) {
                     // byte k -> 2^23 + byte (PRMT into the mantissa), then one packed add
 #pragma unroll
                     for (int q = 0; q < NP; ++q) {
-                        const unsigned f0 = __byte_perm(raw[u], 0x4B000000u, 0x7440 | (2 * q));
-                        const unsigned f1 = __byte_perm(raw[u], 0x4B000000u, 0x7440 | (2 * q + 1));
+                        const unsigned f0 = __byte_perm(v, 0x4B000000u, 0x7440 | (2 * q));
+                        const unsigned f1 = __byte_perm(v, 0x4B000000u, 0x7440 | (2 * q + 1));
                         x[q] = fadd2p(((f2p)f1 << 32) | f0, mbias);
                     }
                 } else {
-                    x[0] = ((f2p)raw[u].y << 32) | raw[u].x;
+                    x[0] = ((f2p)v.y << 32) | v.x;
                 }
-                raw[u] = fetch(t + K);
-                const bool const_row = a.border == IPFC_BORDER_CONSTANT && (unsigned)(ybase + t) >= (unsigned)a.H;
-                if (const_row || cmask) {
+                raw[u] = fetch(t + K, u);
+                const bool const_row = (unsigned)(ybase + t) >= (unsigned)a.H;
+                if (cfix && (const_row || cmask)) {
 #pragma unroll
                     for (int q = 0; q < NP; ++q) {
                         float2 v = upk2(x[q]);

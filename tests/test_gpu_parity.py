@@ -290,3 +290,34 @@ def test_medium_all_borders_u8(gpu, orc, c, w):
     from imageprocessingflex_b200 import _lib
 
     assert _lib.load().ipfc_check_device(None) == 0
+
+
+@pytest.mark.parametrize("c,dt", [(1, np.uint8), (3, np.uint8), (4, np.uint8), (1, np.float32)],
+                         ids=["u8c1", "u8c3", "u8c4", "f32c1"])
+def test_sep_border_lanes_every_row_residue(gpu, orc, c, dt):
+    """The fast separable kernel's load plan: lanes whose samples are border
+    mapped or straddle the row end assemble them from up to three aligned
+    words; unaligned sources load sample by sample.  Widths with every row
+    length mod 4, one strip and several, every border, host arrays (pitch
+    padded to 128 B), contiguous device tensors (pitch = row length) and a
+    view one pixel in (unaligned base).  Integer taps make the u8 bar exact."""
+    import torch
+
+    B = gpu.BorderMode
+    rng = np.random.default_rng(11 * c + (dt == np.float32))
+    widths = [1, 2, 3, 5, 6, 7, 8, 9, 30, 31, 33, 34, 313, 314, 315, 316, 629, 630, 631, 633, 1001, 1002]
+    ks = (5, 13, 17) if dt == np.float32 else (5, 13, 25)
+    for w in widths:
+        img = oracle.random_image(w + 1, 23, c, dt, 1000 * c + w)
+        host = np.ascontiguousarray(img[:, 1:])
+        dev = torch.from_numpy(host).cuda()
+        view = torch.from_numpy(img).cuda()[:, 1:]
+        for k in ks:
+            kx = rng.integers(-3, 4, size=k).astype(np.float64)
+            ky = rng.integers(-3, 4, size=k).astype(np.float64)
+            for b in oracle.BORDERS:
+                want = orc.sep_filter(host, kx, ky, border=b, delta=0.0, border_value=2.0)
+                tol = G.tolerance("sep", {"border_value": 2.0, "delta": 0.0}, {"src": host, "kx": kx, "ky": ky}, want)
+                G.compare(gpu.sepFilter2D(host, kx, ky, B(b), 0.0, 2.0), want, tol)
+                G.compare(gpu.sepFilter2D(dev, kx, ky, B(b), 0.0, 2.0).cpu().numpy(), want, tol)
+                G.compare(gpu.sepFilter2D(view, kx, ky, B(b), 0.0, 2.0).cpu().numpy(), want, tol)
