@@ -14,8 +14,10 @@
 //    accumulator pairs in registers with fma.rn.f32x2 (one instruction per
 //    two samples; every ring index is a compile-time constant).  Each row's
 //    samples are loaded K rows ahead of use through the read-only path (one
-//    32-bit load per thread for 8-bit sources), border columns resolved per
-//    thread, border rows through a non-inlined slow path.
+//    32-bit load per thread for 8-bit sources, the same instruction in every
+//    lane); lanes with border-mapped samples add up to two cp.async word
+//    copies per row and assemble their bytes at use; border rows resolve
+//    through a non-inlined slow path.
 //  * Finished column-pass rows go to shared memory split by channel
 //    (planar), TB = K rows per band.  Then the CTA switches to the row
 //    pass: one thread per (band row, run of RUN output pixels) reads its
