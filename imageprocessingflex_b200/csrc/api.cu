@@ -324,6 +324,8 @@ bool make_sep_fast_args(const ipfc_image* src, const ipfc_image* dst, const void
                         void* out_ptr, long long out_pitch, const double* kx, int kw, const double* ky, int kh, int ax,
                         int ay, int border, double delta, double bv, SepFastArgs* fp) {
     if (!sep_fast_eligible(src, kx, kw, ky, kh, ax, ay)) return false;
+    // the kernel forms row offsets as 32 x 32-bit products
+    if (in_pitch <= 0 || in_pitch >= (1LL << 31) || out_pitch <= 0 || out_pitch >= (1LL << 31)) return false;
     SepFastArgs& f = *fp;
     std::memset(&f, 0, sizeof(f));
     f.src = in_ptr;

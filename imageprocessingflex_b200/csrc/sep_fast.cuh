@@ -90,8 +90,9 @@ struct FastGeom {
     static constexpr int RUNS = PX / RUN;
     static constexpr int VW = PX + HX;        // plane row width (pixels)
     // row stride = 4 (mod 32) floats: lanes reading 16 B at the same column
-    // of consecutive rows hit distinct 16-byte bank groups
-    static constexpr int VW4 = (VW + 3) / 4 * 4;
+    // of consecutive rows hit distinct 16-byte bank groups.  Column VW is
+    // always padding: lanes without a column store there.
+    static constexpr int VW4 = (VW + 1 + 3) / 4 * 4;
     static constexpr int VWP = VW4 + ((4 - VW4 % 32) + 32) % 32;
     static constexpr int PLANE = TB * VWP;
     static constexpr size_t PLANES_BYTES = sizeof(float) * (size_t)C * PLANE;
@@ -252,8 +253,9 @@ __device__ __forceinline__ void sep_row_pass(const SepFastArgs& a, const float* 
         if (y >= a.H) continue;
         const int px = x0 + p0;
         constexpr int NBYTES = G::RUN * C * (int)sizeof(Tout);
-        unsigned char* db =
-            reinterpret_cast<unsigned char*>(row_ptr_mut<Tout>(a.dst, a.dpitch, y)) + (size_t)px * C * sizeof(Tout);
+        // one 32 x 32 -> 64-bit multiply-add (pitches are below 2^31)
+        unsigned char* db = static_cast<unsigned char*>(a.dst) + (size_t)(unsigned)(px * C * (int)sizeof(Tout)) +
+                            (unsigned long long)(unsigned)y * (unsigned)a.dpitch;
         if (px + G::RUN <= a.W && a.vec_store) {
             if constexpr (NBYTES % 16 == 0) {
 #pragma unroll
@@ -391,11 +393,14 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
 #pragma unroll
     for (int k = 0; k < NCOL; ++k) idx[k] = max(idx[k], 0);
     unsigned* xring = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(vbuf) + G::PLANES_BYTES) + tid;
-    int vdst[NCOL];  // shared offset of this column in band row 0 (-1: not stored)
+    const unsigned char* cbase = static_cast<const unsigned char*>(a.src) + (size_t)c0 * sizeof(Tin);
+    // Shared offset of each column in band row 0; a lane without that column
+    // stores into the padding column (never read as a window value).
+    int vdst[NCOL];
 #pragma unroll
     for (int k = 0; k < NCOL; ++k) {
         const int s = s0 + k;
-        vdst[k] = (active && s >= 0 && s < G::IW) ? (s % C) * G::PLANE + s / C : -1;
+        vdst[k] = (active && s >= 0 && s < G::IW) ? (s % C) * G::PLANE + s / C : G::VW;
     }
 
     f2p acc[K][NP];
@@ -406,8 +411,11 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
 
     const int T = nrows + K - 1;                   // source rows walked
     const int ybase = r0 - K / 2;                  // image row of source row 0
-    int band_row = 0;                              // rows filled in the band buffer
     int band_start = r0;                           // image row of band row 0
+    // Output i (source row t = K-1+i, ring step u = t mod K) goes to band row
+    // i mod TB = (u + 1) mod K: TB = K, so every store offset is a
+    // compile-time constant, and band m is full at step u = K-2, t = (m+2)K-2.
+    static_assert(G::TB == K, "band rows follow the ring");
 
     // ------------------------------------------------------------- column pass
     // The raw samples of the next K rows, loaded K rows ahead of use.
@@ -420,14 +428,21 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
     auto fetch = [&](int t, int slot) -> Raw {
         Raw r{};
         if (t < T) {
-            const Tin* srow = row_ptr<Tin>(a.src, a.spitch, row_any(ybase + t, a.H, a.border));
+            // row address: one 32 x 32 -> 64-bit multiply-add onto the lane's
+            // own base (pitches are below 2^31)
+            const unsigned sy = (unsigned)row_any(ybase + t, a.H, a.border);
             if (!wbytes) {
+                const unsigned char* p = cbase + (unsigned long long)sy * (unsigned)a.spitch;
                 if constexpr (sizeof(Tin) == 1) {
-                    r = __ldg(reinterpret_cast<const unsigned*>(srow + c0));
+                    r = __ldg(reinterpret_cast<const unsigned*>(p));
                 } else {
-                    const float2 v = __ldg(reinterpret_cast<const float2*>(srow + c0));
+                    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
                     r = make_uint2(__float_as_uint(v.x), __float_as_uint(v.y));
                 }
+            }
+            const Tin* srow = reinterpret_cast<const Tin*>(static_cast<const unsigned char*>(a.src) +
+                                                           (unsigned long long)sy * (unsigned)a.spitch);
+            if (!wbytes) {
                 if (wextra) {
                     cp_async4(xring + (2 * slot) * kFastThreads, srow + c1, n1);
                     cp_async4(xring + (2 * slot + 1) * kFastThreads, srow + c2, n2);
@@ -471,14 +486,16 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
                     x[0] = ((f2p)v.y << 32) | v.x;
                 }
                 raw[u] = fetch(t + K, u);
-                const bool const_row = (unsigned)(ybase + t) >= (unsigned)a.H;
-                if (cfix && (const_row || cmask)) {
+                if (cfix) {
+                    const bool const_row = (unsigned)(ybase + t) >= (unsigned)a.H;
+                    if (const_row || cmask) {
 #pragma unroll
-                    for (int q = 0; q < NP; ++q) {
-                        float2 v = upk2(x[q]);
-                        if (const_row || ((cmask >> (2 * q)) & 1u)) v.x = a.bv;
-                        if (const_row || ((cmask >> (2 * q + 1)) & 1u)) v.y = a.bv;
-                        x[q] = pk2(v.x, v.y);
+                        for (int q = 0; q < NP; ++q) {
+                            float2 v = upk2(x[q]);
+                            if (const_row || ((cmask >> (2 * q)) & 1u)) v.x = a.bv;
+                            if (const_row || ((cmask >> (2 * q + 1)) & 1u)) v.y = a.bv;
+                            x[q] = pk2(v.x, v.y);
+                        }
                     }
                 }
                 // source row t feeds output o = t - j with tap j (ring slot (u - j) mod K)
@@ -488,31 +505,28 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
 #pragma unroll
                     for (int q = 0; q < NP; ++q) acc[slot][q] = ffma2p(a.ky2[j], x[q], acc[slot][q]);
                 });
-                constexpr int done = (u + 1) % K;  // slot of output t - (K - 1)
+                constexpr int done = (u + 1) % K;  // slot of output t - (K - 1), and its band row
                 if (t >= K - 1) {
-                    const int off = band_row * G::VWP;
+                    constexpr int off = done * G::VWP;
 #pragma unroll
                     for (int q = 0; q < NP; ++q) {
-                        if (vdst[2 * q] >= 0) vbuf[vdst[2 * q] + off] = lo_f(acc[done][q]);
-                        if (vdst[2 * q + 1] >= 0) vbuf[vdst[2 * q + 1] + off] = hi_f(acc[done][q]);
+                        vbuf[vdst[2 * q] + off] = lo_f(acc[done][q]);
+                        vbuf[vdst[2 * q + 1] + off] = hi_f(acc[done][q]);
                     }
-                    ++band_row;
                 }
 #pragma unroll
                 for (int q = 0; q < NP; ++q) acc[done][q] = 0ull;
-                // TB is a multiple of K and the first output leaves at t = K-1,
-                // so a band always fills at ring position u = K-2.
                 if constexpr (u == K - 2) {
-                    if (band_row == G::TB) {
+                    if (t >= 2 * K - 2) {
                         sep_row_pass<K, C, Tout, G>(a, vbuf, G::TB, band_start, x0);
                         band_start += G::TB;
-                        band_row = 0;
                     }
                 }
             }
         });
     }
-    if (band_row > 0) sep_row_pass_cold<K, C, Tout, G>(a, vbuf, band_row, band_start, x0);
+    const int rem = nrows % G::TB;  // outputs of the last, partial band
+    if (rem > 0) sep_row_pass_cold<K, C, Tout, G>(a, vbuf, rem, band_start, x0);
 }
 
 // ---- the kernel: one tile per CTA --------------------------------------------
