@@ -479,7 +479,7 @@ def run_batch(args):
                    "timing": "CUDA events on the launching stream"},
         "gpu_launches": kernels * args.steps,
         "batched": {"ms": round(ms_batched, 4), "mpix_s": round(mpix / (ms_batched / 1e3), 1),
-                    "kernels_per_step": kernels, "tiles": b.info("tiles_light") + b.info("tiles_heavy"),
+                    "kernels_per_step": kernels, "tiles": b.info("tiles_light") + b.info("tiles_heavy") + b.info("tiles_mem"),
                     "plan_seconds": round(t_plan, 3)},
         "plain": {"ms": round(ms_plain, 4), "mpix_s": round(mpix / (ms_plain / 1e3), 1),
                   "launches_per_step": len(items), "form": "one C-ABI call per image from the host"},

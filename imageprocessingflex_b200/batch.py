@@ -22,7 +22,7 @@ from .filters import BorderMode, Error, _check, _f64, _is_tensor, _stream_of, _v
 
 AUTOTUNE, GRAPH = 1, 2
 INFO = {"items": 0, "planned": 1, "tiles_light": 2, "tiles_heavy": 3, "grid_light": 4, "grid_heavy": 5,
-        "kernels": 6, "graph": 7}
+        "kernels": 6, "graph": 7, "tiles_mem": 8, "grid_mem": 9}
 OP_SEP, OP_MEDIAN, OP_MORPH = 0, 1, 2
 
 

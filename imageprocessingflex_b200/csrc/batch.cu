@@ -49,17 +49,22 @@ bool make_sep_fast_args(const ipfc_image* src, const ipfc_image* dst, const void
                         int ay, int border, double delta, double bv, SepFastArgs* fp);
 cudaError_t batch_launch_light(const BatchItem*, const BatchTile*, int, unsigned*, int, size_t, cudaStream_t);
 cudaError_t batch_launch_heavy(const BatchItem*, const BatchTile*, int, unsigned*, int, size_t, cudaStream_t);
+cudaError_t batch_launch_mem(const BatchItem*, const BatchTile*, int, unsigned*, int, size_t, cudaStream_t);
 cudaError_t batch_occupancy_light(size_t smem, int* occ);
 cudaError_t batch_occupancy_heavy(size_t smem, int* occ);
+cudaError_t batch_occupancy_mem(size_t smem, int* occ);
 
 cudaError_t batch_launch(int cls, const BatchItem* items, const BatchTile* tiles, int ntiles, unsigned* counter,
                          int grid, size_t smem, cudaStream_t s) {
-    return cls == 0 ? batch_launch_light(items, tiles, ntiles, counter, grid, smem, s)
-                    : batch_launch_heavy(items, tiles, ntiles, counter, grid, smem, s);
+    if (cls == kBatchLight) return batch_launch_light(items, tiles, ntiles, counter, grid, smem, s);
+    if (cls == kBatchHeavy) return batch_launch_heavy(items, tiles, ntiles, counter, grid, smem, s);
+    return batch_launch_mem(items, tiles, ntiles, counter, grid, smem, s);
 }
 
 cudaError_t batch_occupancy(int cls, size_t smem, int* occ) {
-    return cls == 0 ? batch_occupancy_light(smem, occ) : batch_occupancy_heavy(smem, occ);
+    if (cls == kBatchLight) return batch_occupancy_light(smem, occ);
+    if (cls == kBatchHeavy) return batch_occupancy_heavy(smem, occ);
+    return batch_occupancy_mem(smem, occ);
 }
 
 namespace {
@@ -93,7 +98,11 @@ std::vector<TuneVal> candidates(int kind, int k) {
 
 TuneVal default_val(int kind, int k) { return kind == kBatchSep ? TuneVal{8 * k, 0} : TuneVal{128, 32}; }
 
-int batch_class(int kind, int k) { return (kind == kBatchSep && k > kBatchLightMaxTaps) ? 1 : 0; }
+int batch_class(int kind, int k) {
+    if (kind == kBatchSep) return k > kBatchLightMaxTaps ? kBatchHeavy : kBatchLight;
+    if (kind == kBatchMedian) return (k == 3 || k == 5) ? kBatchMem : kBatchLight;
+    return kBatchMem;  // morphology
+}
 
 struct Tiling {
     int cls = 0;
@@ -139,7 +148,7 @@ struct Plan {
     BatchItem* d_items = nullptr;
     BatchTile* d_tiles = nullptr;
     unsigned* d_counter = nullptr;
-    int grid[kBatchClasses] = {0, 0};
+    int grid[kBatchClasses] = {};
 
     void release() {
         if (d_items) cudaFree(d_items);
@@ -202,24 +211,36 @@ cudaError_t plan_grids(const HostPlan& p, int grid[kBatchClasses]) {
 }
 
 cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsigned* d_counter, const HostPlan& p,
-                        const int grid[kBatchClasses], cudaStream_t s0, cudaStream_t s1, cudaEvent_t fork,
-                        cudaEvent_t join) {
+                        const int grid[kBatchClasses], cudaStream_t s0, cudaStream_t s1, cudaStream_t s2,
+                        cudaEvent_t fork, cudaEvent_t join) {
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * kBatchClasses, s0);
     if (e != cudaSuccess) return e;
-    const bool both = p.ntiles[0] > 0 && p.ntiles[1] > 0 && s1;
-    if (both) {
-        if ((e = cudaEventRecord(fork, s0)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(s1, fork, 0)) != cudaSuccess) return e;
-    }
-    // heavy first: its tiles are the longest
-    for (int c = kBatchClasses - 1; c >= 0; --c) {
+    // Launch order: the heavy class (longest tiles), then the memory-bound
+    // class (its CTAs fit on the SMs beside heavy ones), then the light class.
+    // With side streams each class after the first gets its own branch.
+    const int order[kBatchClasses] = {kBatchHeavy, kBatchMem, kBatchLight};
+    const cudaStream_t lane[kBatchClasses] = {s0, s1, s2};
+    int nonempty = 0;
+    for (int c = 0; c < kBatchClasses; ++c) nonempty += p.ntiles[c] > 0;
+    const bool branches = s1 && s2 && fork && join && nonempty > 1;
+    // the fork follows the counter reset and precedes every launch
+    if (branches && (e = cudaEventRecord(fork, s0)) != cudaSuccess) return e;
+    int used = 0;
+    for (int i = 0; i < kBatchClasses; ++i) {
+        const int c = order[i];
         if (p.ntiles[c] == 0) continue;
-        cudaStream_t s = (both && c == 0) ? s1 : s0;
+        cudaStream_t s = s0;
+        if (branches && used > 0) {
+            s = lane[used];
+            if ((e = cudaStreamWaitEvent(s, fork, 0)) != cudaSuccess) return e;
+        }
         e = batch_launch(c, d_items, d_tiles + p.tile_off[c], p.ntiles[c], d_counter + c, grid[c], p.smem[c], s);
         if (e != cudaSuccess) return e;
+        ++used;
     }
-    if (both) {
-        if ((e = cudaEventRecord(join, s1)) != cudaSuccess) return e;
+    // join: s0 waits for each branch (the event is re-recorded per branch)
+    for (int b = 1; branches && b < used; ++b) {
+        if ((e = cudaEventRecord(join, lane[b])) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(s0, join, 0)) != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -256,9 +277,10 @@ cudaError_t make_plan(const std::vector<HostItem>& items, const std::vector<Tune
 }
 
 // Enqueues one execution of a plan: counter reset, then the classes' kernels
-// (on s0, or as two parallel branches when s1 and the events are given).
-cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, cudaStream_t s1, cudaEvent_t fork, cudaEvent_t join) {
-    return launch_plan(p.d_items, p.d_tiles, p.d_counter, p.host, p.grid, s0, s1, fork, join);
+// (on s0, or as parallel branches when s1, s2 and the events are given).
+cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, cudaStream_t s1, cudaStream_t s2, cudaEvent_t fork,
+                         cudaEvent_t join) {
+    return launch_plan(p.d_items, p.d_tiles, p.d_counter, p.host, p.grid, s0, s1, s2, fork, join);
 }
 
 // Times candidate tile shapes for one key on synthetic images; returns the
@@ -328,7 +350,7 @@ cudaError_t tune_key(const TuneKey& key, const HostItem& proto, TuneVal* best) {
         float ms = 1e30f;
         for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
             e = cudaEventRecord(t0, s);
-            if (e == cudaSuccess) e = enqueue_plan(p, s, nullptr, nullptr, nullptr);
+            if (e == cudaSuccess) e = enqueue_plan(p, s, nullptr, nullptr, nullptr, nullptr);
             if (e == cudaSuccess) e = cudaEventRecord(t1, s);
             if (e == cudaSuccess) e = cudaEventSynchronize(t1);
             float m = 0;
@@ -366,8 +388,8 @@ struct ipfc_batch {
     int device = -1;
     bool planned = false;
     Plan plan;
-    cudaStream_t st[2] = {nullptr, nullptr};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaStream_t st[3] = {nullptr, nullptr, nullptr};  // capture stream and two branches
+    cudaEvent_t ev[2] = {nullptr, nullptr};            // fork, join
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 
@@ -381,10 +403,10 @@ struct ipfc_batch {
     }
     ~ipfc_batch() {
         drop_plan();
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < 3; ++i)
             if (st[i]) cudaStreamDestroy(st[i]);
+        for (int i = 0; i < 2; ++i)
             if (ev[i]) cudaEventDestroy(ev[i]);
-        }
     }
 };
 
@@ -474,14 +496,14 @@ int plan_batch(ipfc_batch* b, const char* fn) {
     }
     e = make_plan(b->items, vals, &b->plan);
     if (e != cudaSuccess) return cuda_status(e, fn);
-    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i)
         if (!b->st[i]) e = cudaStreamCreateWithFlags(&b->st[i], cudaStreamNonBlocking);
-        if (e == cudaSuccess && !b->ev[i]) e = cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming);
-    }
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+        if (!b->ev[i]) e = cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming);
     if (e == cudaSuccess && b->use_graph) {
         e = cudaStreamBeginCapture(b->st[0], cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            cudaError_t e2 = enqueue_plan(b->plan, b->st[0], b->st[1], b->ev[0], b->ev[1]);
+            cudaError_t e2 = enqueue_plan(b->plan, b->st[0], b->st[1], b->st[2], b->ev[0], b->ev[1]);
             e = cudaStreamEndCapture(b->st[0], &b->graph);
             if (e2 != cudaSuccess) e = e2;
         }
@@ -619,7 +641,7 @@ int ipfc_batch_run(ipfc_batch* b, void* stream) {
     if (b->exec) {
         e = cudaGraphLaunch(b->exec, s);
     } else {
-        e = enqueue_plan(b->plan, s, nullptr, nullptr, nullptr);
+        e = enqueue_plan(b->plan, s, nullptr, nullptr, nullptr, nullptr);
     }
     return e == cudaSuccess ? IPFC_OK : cuda_status(e, fn);
 }
@@ -630,11 +652,16 @@ int ipfc_batch_info(const ipfc_batch* b, int what, long long* value) {
     switch (what) {
         case IPFC_BATCH_INFO_ITEMS: *value = (long long)b->items.size(); break;
         case IPFC_BATCH_INFO_PLANNED: *value = b->planned ? 1 : 0; break;
-        case IPFC_BATCH_INFO_TILES_LIGHT: *value = p.host.ntiles[0]; break;
-        case IPFC_BATCH_INFO_TILES_HEAVY: *value = p.host.ntiles[1]; break;
-        case IPFC_BATCH_INFO_GRID_LIGHT: *value = p.grid[0]; break;
-        case IPFC_BATCH_INFO_GRID_HEAVY: *value = p.grid[1]; break;
-        case IPFC_BATCH_INFO_KERNELS: *value = (p.host.ntiles[0] > 0) + (p.host.ntiles[1] > 0); break;
+        case IPFC_BATCH_INFO_TILES_LIGHT: *value = p.host.ntiles[kBatchLight]; break;
+        case IPFC_BATCH_INFO_TILES_HEAVY: *value = p.host.ntiles[kBatchHeavy]; break;
+        case IPFC_BATCH_INFO_TILES_MEM: *value = p.host.ntiles[kBatchMem]; break;
+        case IPFC_BATCH_INFO_GRID_LIGHT: *value = p.grid[kBatchLight]; break;
+        case IPFC_BATCH_INFO_GRID_HEAVY: *value = p.grid[kBatchHeavy]; break;
+        case IPFC_BATCH_INFO_GRID_MEM: *value = p.grid[kBatchMem]; break;
+        case IPFC_BATCH_INFO_KERNELS:
+            *value = 0;
+            for (int c = 0; c < kBatchClasses; ++c) *value += p.host.ntiles[c] > 0;
+            break;
         case IPFC_BATCH_INFO_GRAPH: *value = b->exec ? 1 : 0; break;
         default: return set_error(IPFC_ERR_INVALID, "ipf: batch: unknown info %d", what);
     }

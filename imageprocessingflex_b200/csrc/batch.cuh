@@ -15,9 +15,11 @@
 //
 // Register classes: the tile bodies differ a lot in registers and shared
 // memory, and a kernel is launched with the largest need of everything it
-// can run.  Light tiles (separable K <= 13, median, morphology) run two CTAs
-// per SM; heavy tiles (separable K 15..25) one.  Each class is its own
-// persistent kernel with its own queue.
+// can run.  Light tiles (separable K <= 13, median k >= 7) run two CTAs per
+// SM; heavy tiles (separable K 15..25) one; memory-bound tiles (3x3 and 5x5
+// median, morphology) at least four, with 64 registers a thread, so that
+// many tiles' loads are in flight and their CTAs fit beside a heavy one.
+// Each class is its own persistent kernel with its own queue.
 #pragma once
 
 #include "median.cuh"
@@ -30,7 +32,8 @@ namespace ipfc {
 
 enum BatchKind { kBatchSep = 0, kBatchMedian = 1, kBatchMorph = 2 };
 
-constexpr int kBatchClasses = 2;
+constexpr int kBatchClasses = 3;
+constexpr int kBatchLight = 0, kBatchHeavy = 1, kBatchMem = 2;
 constexpr int kBatchLightMaxTaps = 13;
 constexpr int kBatchMaxTaps = 25;
 

@@ -21,11 +21,13 @@ __device__ __noinline__ void batch_sep_tile(int x, int y) {
 }
 
 static __device__ __noinline__ void batch_median_tile(int x, int y) {
-    if (g_batch_item.K == 3 || g_batch_item.K == 5)
-        median_u8_tile(g_batch_item.u.med, g_batch_item.tx, g_batch_item.ty, x, y,
-                       reinterpret_cast<unsigned char*>(g_batch_smem));
-    else
-        median_tile<uint8_t>(g_batch_item.u.med, g_batch_item.tx, g_batch_item.ty, x, y, g_batch_smem);
+    median_tile<uint8_t>(g_batch_item.u.med, g_batch_item.tx, g_batch_item.ty, x, y, g_batch_smem);
+}
+
+// 3x3 and 5x5 (the memory-bound class)
+static __device__ __noinline__ void batch_median_u8_tile(int x, int y) {
+    median_u8_tile(g_batch_item.u.med, g_batch_item.tx, g_batch_item.ty, x, y,
+                   reinterpret_cast<unsigned char*>(g_batch_smem));
 }
 
 static __device__ __noinline__ void batch_morph_tile(int x, int y) {
@@ -45,15 +47,16 @@ __device__ __forceinline__ bool batch_sep_case(int k, int c, int x, int y) {
 
 template <int CLS>
 __device__ __forceinline__ void batch_run_tile(int kind, int k, int c, int x, int y) {
-    if constexpr (CLS == 0) {
+    if constexpr (CLS == kBatchLight) {
         if (kind == kBatchSep) {
             batch_sep_case<3>(k, c, x, y) || batch_sep_case<5>(k, c, x, y) || batch_sep_case<7>(k, c, x, y) ||
                 batch_sep_case<9>(k, c, x, y) || batch_sep_case<11>(k, c, x, y) || batch_sep_case<13>(k, c, x, y);
-        } else if (kind == kBatchMedian) {
-            batch_median_tile(x, y);
         } else {
-            batch_morph_tile(x, y);
+            batch_median_tile(x, y);
         }
+    } else if constexpr (CLS == kBatchMem) {
+        if (kind == kBatchMedian) batch_median_u8_tile(x, y);
+        else batch_morph_tile(x, y);
     } else {
         batch_sep_case<15>(k, c, x, y) || batch_sep_case<17>(k, c, x, y) || batch_sep_case<19>(k, c, x, y) ||
             batch_sep_case<21>(k, c, x, y) || batch_sep_case<23>(k, c, x, y) || batch_sep_case<25>(k, c, x, y);
@@ -63,7 +66,7 @@ __device__ __forceinline__ void batch_run_tile(int kind, int k, int c, int x, in
 // The tile loop.  Thread 0 takes the next tile index; the whole CTA reads it
 // after a barrier, so every exit and item switch is CTA-uniform.
 template <int CLS>
-__global__ void __launch_bounds__(kFastThreads, CLS == 0 ? 2 : 1)
+__global__ void __launch_bounds__(kFastThreads, CLS == kBatchLight ? 2 : CLS == kBatchHeavy ? 1 : 4)
     batch_kernel(const BatchItem* __restrict__ items, const BatchTile* __restrict__ tiles, int ntiles,
                  unsigned* __restrict__ counter) {
     __shared__ int next;
@@ -102,6 +105,11 @@ cudaError_t batch_prepare_class() {
     if ((e = cudaFuncGetAttributes(&fa, (const void*)batch_kernel<CLS>)) != cudaSuccess) return e;
     e = cudaFuncSetAttribute((const void*)batch_kernel<CLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              optin - (int)fa.sharedSizeBytes);
+    // Every class asks for the same (largest) shared-memory carveout, so that
+    // memory-bound CTAs can share an SM with a heavy CTA that is running.
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute((const void*)batch_kernel<CLS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess) __atomic_fetch_or(&done, bit, __ATOMIC_ACQ_REL);
     return e;
 }

@@ -21,15 +21,16 @@ struct HostItem {
     int W = 0, H = 0;
 };
 
-// Items with their tile parameters applied, and the tile list: class 0
-// (light) tiles first, each class ordered by estimated cost per tile.
+// Items with their tile parameters applied, and the tile list grouped by
+// class (light, heavy, memory-bound), each class ordered by estimated cost
+// per tile.
 struct HostPlan {
     std::vector<BatchItem> items;
     std::vector<BatchTile> tiles;
-    int ntiles[kBatchClasses] = {0, 0};
-    int tile_off[kBatchClasses] = {0, 0};
-    size_t smem[kBatchClasses] = {0, 0};
-    double cost[kBatchClasses] = {0, 0};
+    int ntiles[kBatchClasses] = {};
+    int tile_off[kBatchClasses] = {};
+    size_t smem[kBatchClasses] = {};
+    double cost[kBatchClasses] = {};
 };
 
 void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneVal>& vals, HostPlan* p);
@@ -39,11 +40,11 @@ void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneV
 cudaError_t plan_grids(const HostPlan& p, int grid[kBatchClasses]);
 
 // Enqueues the plan whose items and tiles are in device memory: resets the
-// two counters, then launches the classes on s0 (or as parallel branches
-// on s0 and s1 when s1, fork and join are given).
+// class counters, then launches the classes on s0 (or as parallel branches
+// on s0, s1 and s2 when the side streams, fork and join are all given).
 cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsigned* d_counter, const HostPlan& p,
-                        const int grid[kBatchClasses], cudaStream_t s0, cudaStream_t s1, cudaEvent_t fork,
-                        cudaEvent_t join);
+                        const int grid[kBatchClasses], cudaStream_t s0, cudaStream_t s1, cudaStream_t s2,
+                        cudaEvent_t fork, cudaEvent_t join);
 
 // Tile parameters for an item: the autotuner's entry for its key on the
 // current device, else the built-in default.  Never tunes.
