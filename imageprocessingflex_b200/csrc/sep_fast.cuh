@@ -36,6 +36,9 @@ namespace ipfc {
 
 constexpr int kFastThreads = 256;
 constexpr int kFastMaxTaps = 32;
+// Up to this many taps two CTAs share an SM (128 registers a thread); longer
+// kernels need more registers for the K-deep accumulator ring and run one.
+constexpr int kFastTwoCtaTaps = 15;
 
 struct SepFastArgs {
     const void* src;
@@ -531,7 +534,7 @@ __device__ __forceinline__ void sep_fast_tile(const SepFastArgs& a, float* vbuf,
 
 // ---- the kernel: one tile per CTA --------------------------------------------
 template <int K, int C, typename Tin, typename Tout>
-__global__ void __launch_bounds__(kFastThreads, (K <= 17 ? 2 : 1))
+__global__ void __launch_bounds__(kFastThreads, (K <= kFastTwoCtaTaps ? 2 : 1))
     sep_fast_kernel(const __grid_constant__ SepFastArgs a) {
     extern __shared__ __align__(128) float vbuf[];  // C planes x TB rows x VWP
     sep_fast_tile<K, C, Tin, Tout>(a, vbuf, blockIdx.x % a.strips, blockIdx.x / a.strips);
