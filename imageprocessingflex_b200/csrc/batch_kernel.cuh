@@ -105,11 +105,6 @@ cudaError_t batch_prepare_class() {
     if ((e = cudaFuncGetAttributes(&fa, (const void*)batch_kernel<CLS>)) != cudaSuccess) return e;
     e = cudaFuncSetAttribute((const void*)batch_kernel<CLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              optin - (int)fa.sharedSizeBytes);
-    // Every class asks for the same (largest) shared-memory carveout, so that
-    // memory-bound CTAs can share an SM with a heavy CTA that is running.
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute((const void*)batch_kernel<CLS>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess) __atomic_fetch_or(&done, bit, __ATOMIC_ACQ_REL);
     return e;
 }
