@@ -93,7 +93,7 @@ const int kClassSide[kSizeClasses] = {192, 512, 1024, 2048};
 
 std::vector<TuneVal> candidates(int kind, int k) {
     if (kind == kBatchSep) return {{2 * k, 0}, {4 * k, 0}, {8 * k, 0}, {16 * k, 0}};
-    return {{128, 16}, {128, 32}, {256, 16}, {256, 32}};
+    return {{128, 16}, {128, 32}, {256, 16}, {256, 32}, {256, 64}};
 }
 
 TuneVal default_val(int kind, int k) { return kind == kBatchSep ? TuneVal{8 * k, 0} : TuneVal{128, 32}; }
@@ -289,44 +289,47 @@ cudaError_t tune_key(const TuneKey& key, const HostItem& proto, TuneVal* best) {
     const int side = kClassSide[key.size_class];
     const int W = side, H = side, C = key.c;
     const long long bytes = (long long)W * H * C;
-    // enough copies to fill the device several times over
-    const int copies = (int)std::max(4LL, std::min(64LL, (64LL << 20) / std::max(1LL, bytes)));
+    // Enough copies to fill the device several times over, each with its own
+    // source and destination: the 256 MB or more they span is beyond L2, so
+    // memory-bound tiles are timed reading DRAM as a real batch does.
+    const int copies = (int)std::max(4LL, std::min(1024LL, (256LL << 20) / std::max(1LL, bytes)));
     unsigned char* buf = nullptr;
-    cudaError_t e = cudaMalloc((void**)&buf, (size_t)bytes * 2);
+    cudaError_t e = cudaMalloc((void**)&buf, (size_t)bytes * 2 * copies);
     if (e != cudaSuccess) return e;
     cudaStream_t s = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
-    e = cudaMemset(buf, 0x5a, (size_t)bytes);
+    e = cudaMemset(buf, 0x5a, (size_t)bytes * 2 * copies);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&t0);
     if (e == cudaSuccess) e = cudaEventCreate(&t1);
     std::vector<HostItem> items((size_t)copies, proto);
-    for (HostItem& h : items) {
+    for (size_t i = 0; i < items.size(); ++i) {
+        HostItem& h = items[i];
         h.W = W;
         h.H = H;
         BatchItem& it = h.it;
-        // every copy reads the same source and writes the same destination:
-        // only the time is used
+        unsigned char* src = buf + (size_t)bytes * 2 * i;  // only the time is used
+        unsigned char* dst = src + bytes;
         if (it.kind == kBatchSep) {
-            it.u.sep.src = buf;
+            it.u.sep.src = src;
             it.u.sep.spitch = (long long)W * C;
-            it.u.sep.dst = buf + bytes;
+            it.u.sep.dst = dst;
             it.u.sep.dpitch = (long long)W * C;
             it.u.sep.W = W;
             it.u.sep.H = H;
             it.u.sep.vec_load = 1;
             it.u.sep.vec_store = ((W * C) % 16 == 0) ? 1 : 0;
         } else if (it.kind == kBatchMedian) {
-            it.u.med.src = buf;
+            it.u.med.src = src;
             it.u.med.spitch = (long long)W * C;
-            it.u.med.dst = buf + bytes;
+            it.u.med.dst = dst;
             it.u.med.dpitch = (long long)W * C;
             it.u.med.W = W;
             it.u.med.H = H;
         } else {
-            it.u.morph.src = buf;
+            it.u.morph.src = src;
             it.u.morph.spitch = (long long)W * C;
-            it.u.morph.dst = buf + bytes;
+            it.u.morph.dst = dst;
             it.u.morph.dpitch = (long long)W * C;
             it.u.morph.W = W;
             it.u.morph.H = H;
