@@ -17,6 +17,15 @@ namespace ipfc {
 // repeated (period 2n), Reflect101 mirrors without it (period 2n-2, n==1 -> 0),
 // Wrap is periodic.  Works for p arbitrarily far outside [0, n).
 // ---------------------------------------------------------------------------
+// 16-byte asynchronous copy global -> shared, both addresses 16-byte
+// aligned, through L2 only.  No register holds the data, so a thread can
+// have many in flight; cp_async_wait_all() waits for all of its own.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __host__ __device__ __forceinline__ int border_index(int p, int n, int mode) {
     if ((unsigned)p < (unsigned)n) return p;
     if (n <= 0) return -1;

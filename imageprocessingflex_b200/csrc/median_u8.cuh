@@ -6,9 +6,10 @@
 // per channel (order statistics, so any exact selection agrees with the
 // reference's histogram / nth_element).
 //
-//  * staging: each source row of the tile (rows border-mapped) is read with
-//    16-byte loads from the 16-byte-aligned address at or below the row's
-//    first sample, keeping the row's offset (0..15) into its staged copy;
+//  * staging: each source row of the tile (rows border-mapped) is copied
+//    with 16-byte cp.async from the 16-byte-aligned address at or below the
+//    row's first sample, all of a thread's rows in flight at once, keeping
+//    the row's offset (0..15) into its staged copy;
 //    16-byte chunks that leave the row are read byte by byte through the
 //    border mapping (border_sample, channel preserved);
 //  * selection: 4 adjacent samples per 32-bit word.  Each window word (the
@@ -111,10 +112,10 @@ __device__ __forceinline__ void median_u8_tile_k(const MedianArgs& a, int TX, in
         const int gc0 = g0 - d;
         for (int c = lane; c < g.SP / 16; c += 32) {
             const int gc = gc0 + 16 * c;
-            uint4 v;
             if (gc >= 0 && gc + 16 <= rowlen) {
-                v = __ldg(reinterpret_cast<const uint4*>(p + gc));
+                cp_async16(dst + c, p + gc);  // all of this thread's rows in flight at once
             } else {
+                uint4 v;
                 unsigned w[4];
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk) {
@@ -128,46 +129,51 @@ __device__ __forceinline__ void median_u8_tile_k(const MedianArgs& a, int TX, in
                     w[kk] = x;
                 }
                 v = make_uint4(w[0], w[1], w[2], w[3]);
+                dst[c] = v;
             }
-            dst[c] = v;
         }
     }
+    cp_async_wait_all();
     __syncthreads();
 
-    // ---- selection and store
-    for (int it = tid; it < TY * g.TW; it += kMedianU8Threads) {
-        const int y = it / g.TW, t = it - y * g.TW;
-        const int gy = y0 + y, q = q0 + 4 * t;
-        if (gy >= a.H || q >= rowlen) continue;
-        unsigned raw[K * K];
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            const unsigned* w = reinterpret_cast<const unsigned*>(stage + (size_t)(y + j) * g.SP);
-            const int s0 = 4 * t + delta[y + j];
-#pragma unroll
-            for (int i = 0; i < K; ++i) raw[j * K + i] = staged_word(w, s0 + i * C);
-        }
-        unsigned ev[K * K], od[K * K];
-#pragma unroll
-        for (int e = 0; e < K * K; ++e) {
-            ev[e] = lanes_even(raw[e]);
-            od[e] = lanes_odd(raw[e]);
-        }
-        unsigned me, mo;
-        if constexpr (K == 3) {
-            me = median9_2(ev);
-            mo = median9_2(od);
-        } else {
-            me = forgetful_2<K * K>(ev);
-            mo = forgetful_2<K * K>(od);
-        }
-        const unsigned acc = lanes_pack(me, mo);
+    // ---- selection and store (a warp per output row, a lane per word: no index division)
+    for (int y = warp; y < TY; y += nwarp) {
+        const int gy = y0 + y;
+        if (gy >= a.H) break;  // rows only grow with y
         unsigned char* drow = reinterpret_cast<unsigned char*>(a.dst) + (long long)gy * a.dpitch;
-        if (q + 4 <= rowlen && (((uintptr_t)(drow + q)) & 3) == 0) {
-            *reinterpret_cast<unsigned*>(drow + q) = acc;
-        } else {
-            const int n = min(4, rowlen - q);
-            for (int b = 0; b < n; ++b) drow[q + b] = (unsigned char)(acc >> (8 * b));
+        const bool aligned = (((uintptr_t)(drow + q0)) & 3) == 0;  // q0 and 4t are multiples of 4
+        for (int t = lane; t < g.TW; t += 32) {
+            const int q = q0 + 4 * t;
+            if (q >= rowlen) break;
+            unsigned raw[K * K];
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                const unsigned* w = reinterpret_cast<const unsigned*>(stage + (size_t)(y + j) * g.SP);
+                const int s0 = 4 * t + delta[y + j];
+#pragma unroll
+                for (int i = 0; i < K; ++i) raw[j * K + i] = staged_word(w, s0 + i * C);
+            }
+            unsigned ev[K * K], od[K * K];
+#pragma unroll
+            for (int e = 0; e < K * K; ++e) {
+                ev[e] = lanes_even(raw[e]);
+                od[e] = lanes_odd(raw[e]);
+            }
+            unsigned me, mo;
+            if constexpr (K == 3) {
+                me = median9_2(ev);
+                mo = median9_2(od);
+            } else {
+                me = forgetful_2<K * K>(ev);
+                mo = forgetful_2<K * K>(od);
+            }
+            const unsigned acc = lanes_pack(me, mo);
+            if (aligned && q + 4 <= rowlen) {
+                *reinterpret_cast<unsigned*>(drow + q) = acc;
+            } else {
+                const int n = min(4, rowlen - q);
+                for (int b = 0; b < n; ++b) drow[q + b] = (unsigned char)(acc >> (8 * b));
+            }
         }
     }
     __syncthreads();

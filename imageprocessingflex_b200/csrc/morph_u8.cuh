@@ -9,9 +9,11 @@
 // centre.
 //
 // Memory path (the op is bound by HBM bandwidth):
-//  * staging: each source row of the tile is read with 16-byte loads from the
-//    16-byte-aligned address at or below the row's first sample, so rows of
-//    any pitch and alignment load with full-width vector loads; the row's
+//  * staging: each source row of the tile is copied with 16-byte cp.async
+//    from the 16-byte-aligned address at or below the row's first sample, so
+//    rows of any pitch and alignment move in full-width copies, all of a
+//    thread's rows in flight at once (a load then store would wait for each
+//    row in turn); the row's
 //    offset into its staged copy (0..15 bytes) is kept per row.  16-byte
 //    chunks that leave the row are read byte by byte, with the identity
 //    outside the image;
@@ -79,10 +81,13 @@ __device__ __forceinline__ unsigned fold2(unsigned a, unsigned b) {
     return IS_MIN ? umin2(a, b) : umax2(a, b);
 }
 
-template <bool IS_MIN>
+// SW, SH: the window at compile time (3 x 3, the common element), or 0 for
+// the sizes in `a`.
+template <bool IS_MIN, int SW, int SH>
 __device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, int TY, int bx, int by,
                                                    unsigned char* smem) {
-    const MorphU8Geom g(TX, TY, a.sw, a.sh, a.C);
+    const int sw = SW > 0 ? SW : a.sw, sh = SH > 0 ? SH : a.sh;
+    const MorphU8Geom g(TX, TY, sw, sh, a.C);
     unsigned char* stage = smem;
     uint2* hrow = reinterpret_cast<uint2*>(smem + (size_t)g.RY * g.SP);
     int* delta = reinterpret_cast<int*>(hrow + (size_t)g.RY * g.TW);
@@ -109,10 +114,10 @@ __device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, i
         const int gc0 = g0 - d;  // global sample of the first staged chunk's first byte
         for (int c = lane; c < nch; c += 32) {
             const int gc = gc0 + 16 * c;
-            uint4 v;
             if (gc >= 0 && gc + 16 <= rowlen) {
-                v = __ldg(reinterpret_cast<const uint4*>(p + gc));
+                cp_async16(dst + c, p + gc);  // all of this thread's rows in flight at once
             } else {
+                uint4 v;
                 unsigned w[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -126,46 +131,68 @@ __device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, i
                     w[k] = x;
                 }
                 v = make_uint4(w[0], w[1], w[2], w[3]);
+                dst[c] = v;
             }
-            dst[c] = v;
         }
     }
+    cp_async_wait_all();
     __syncthreads();
 
     // ---- row pass: hrow[r][t] = fold over i of staged bytes [4t + i*C + delta_r, +4)
-    for (int it = tid; it < g.RY * g.TW; it += kMorphU8Threads) {
-        const int r = it / g.TW, t = it - r * g.TW;
+    // (a warp per row, a lane per word: no index division)
+    for (int r = warp; r < g.RY; r += nwarp) {
         const unsigned* w = reinterpret_cast<const unsigned*>(stage + (size_t)r * g.SP);
-        const int s0 = 4 * t + delta[r];
-        const unsigned w0 = staged_word(w, s0);
-        unsigned ev = lanes_even(w0), od = lanes_odd(w0);
-        for (int i = 1; i < a.sw; ++i) {
-            const unsigned wi = staged_word(w, s0 + i * C);
-            ev = fold2<IS_MIN>(ev, lanes_even(wi));
-            od = fold2<IS_MIN>(od, lanes_odd(wi));
+        const int dr = delta[r];
+        uint2* hr = hrow + (size_t)r * g.TW;
+        for (int t = lane; t < g.TW; t += 32) {
+            const int s0 = 4 * t + dr;
+            const unsigned w0 = staged_word(w, s0);
+            unsigned ev = lanes_even(w0), od = lanes_odd(w0);
+            auto fold_col = [&](int i) {
+                const unsigned wi = staged_word(w, s0 + i * C);
+                ev = fold2<IS_MIN>(ev, lanes_even(wi));
+                od = fold2<IS_MIN>(od, lanes_odd(wi));
+            };
+            if constexpr (SW > 0) {
+#pragma unroll
+                for (int i = 1; i < SW; ++i) fold_col(i);
+            } else {
+                for (int i = 1; i < sw; ++i) fold_col(i);
+            }
+            hr[t] = make_uint2(ev, od);
         }
-        hrow[it] = make_uint2(ev, od);
     }
     __syncthreads();
 
-    // ---- column pass and store
-    for (int it = tid; it < TY * g.TW; it += kMorphU8Threads) {
-        const int y = it / g.TW, t = it - y * g.TW;
-        const int gy = y0 + y, q = q0 + 4 * t;
-        if (gy >= a.H || q >= rowlen) continue;
-        uint2 h = hrow[it];
-        for (int j = 1; j < a.sh; ++j) {
-            const uint2 hj = hrow[it + j * g.TW];
-            h.x = fold2<IS_MIN>(h.x, hj.x);
-            h.y = fold2<IS_MIN>(h.y, hj.y);
-        }
-        const unsigned acc = lanes_pack(h.x, h.y);
+    // ---- column pass and store (a warp per output row, a lane per word)
+    for (int y = warp; y < TY; y += nwarp) {
+        const int gy = y0 + y;
+        if (gy >= a.H) break;  // rows only grow with y
         unsigned char* drow = reinterpret_cast<unsigned char*>(a.dst) + (long long)gy * a.dpitch;
-        if (q + 4 <= rowlen && (((uintptr_t)(drow + q)) & 3) == 0) {
-            *reinterpret_cast<unsigned*>(drow + q) = acc;
-        } else {
-            const int n = min(4, rowlen - q);
-            for (int b = 0; b < n; ++b) drow[q + b] = (unsigned char)(acc >> (8 * b));
+        const bool aligned = (((uintptr_t)(drow + q0)) & 3) == 0;  // q0 and 4t are multiples of 4
+        const uint2* hr = hrow + (size_t)y * g.TW;
+        for (int t = lane; t < g.TW; t += 32) {
+            const int q = q0 + 4 * t;
+            if (q >= rowlen) break;
+            uint2 h = hr[t];
+            auto fold_row = [&](int j) {
+                const uint2 hj = hr[t + j * g.TW];
+                h.x = fold2<IS_MIN>(h.x, hj.x);
+                h.y = fold2<IS_MIN>(h.y, hj.y);
+            };
+            if constexpr (SH > 0) {
+#pragma unroll
+                for (int j = 1; j < SH; ++j) fold_row(j);
+            } else {
+                for (int j = 1; j < sh; ++j) fold_row(j);
+            }
+            const unsigned acc = lanes_pack(h.x, h.y);
+            if (aligned && q + 4 <= rowlen) {
+                *reinterpret_cast<unsigned*>(drow + q) = acc;
+            } else {
+                const int n = min(4, rowlen - q);
+                for (int b = 0; b < n; ++b) drow[q + b] = (unsigned char)(acc >> (8 * b));
+            }
         }
     }
     __syncthreads();
@@ -173,8 +200,14 @@ __device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, i
 
 __device__ __forceinline__ void morph_u8_tile(const MorphCore& a, int TX, int TY, int bx, int by,
                                               unsigned char* smem) {
-    if (a.is_min) morph_u8_tile_impl<true>(a, TX, TY, bx, by, smem);
-    else morph_u8_tile_impl<false>(a, TX, TY, bx, by, smem);
+    const bool w3 = a.sw == 3 && a.sh == 3;
+    if (a.is_min) {
+        if (w3) morph_u8_tile_impl<true, 3, 3>(a, TX, TY, bx, by, smem);
+        else morph_u8_tile_impl<true, 0, 0>(a, TX, TY, bx, by, smem);
+    } else {
+        if (w3) morph_u8_tile_impl<false, 3, 3>(a, TX, TY, bx, by, smem);
+        else morph_u8_tile_impl<false, 0, 0>(a, TX, TY, bx, by, smem);
+    }
 }
 
 }  // namespace ipfc
