@@ -72,7 +72,10 @@ static long long pitch_of(const ipfc_image* im) { return im->pitch > 0 ? im->pit
 // ---------------------------------------------------------------------------
 // Device memory: stream-ordered allocations from the device's default pool,
 // kept cached by a maximal release threshold (set once per device) so that
-// steady-state calls do not return memory to the driver.
+// steady-state calls do not return memory to the driver.  Reuse across
+// streams through inserted dependencies is off: a call on one stream never
+// waits for another stream's work to reuse its freed staging memory, so
+// callers on several streams overlap their copies and kernels.
 // ---------------------------------------------------------------------------
 static unsigned g_pool_ready = 0;
 
@@ -87,6 +90,9 @@ cudaError_t prepare_device() {
     if (e != cudaSuccess) return e;
     unsigned long long thr = ~0ull;
     e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    if (e != cudaSuccess) return e;
+    int no_internal_deps = 0;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no_internal_deps);
     if (e != cudaSuccess) return e;
     __atomic_fetch_or(&g_pool_ready, bit, __ATOMIC_ACQ_REL);
     return cudaSuccess;
