@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -100,8 +101,10 @@ cudaError_t prepare_device() {
 
 // Device error word: kernels with bounded waits record a code here when a
 // wait gives up.  One word per device, allocated on the first call that
-// launches such a kernel on that device.
+// launches such a kernel on that device (under a lock: callers may be on
+// several threads).
 static unsigned* g_err_word[32] = {nullptr};
+static std::mutex g_err_word_mu;
 
 unsigned* device_error_word() {
     int dev = 0;
@@ -109,6 +112,7 @@ unsigned* device_error_word() {
         cudaGetLastError();
         return nullptr;
     }
+    std::lock_guard<std::mutex> lk(g_err_word_mu);
     unsigned*& w = g_err_word[dev & 31];
     if (!w) {
         unsigned* p = nullptr;
@@ -293,11 +297,10 @@ bool sep_tc_launch(const void* src, long long spitch, void* dst, long long dpitc
 // selects the tensor-core column-pass kernel (sep_tc.cu) where it is
 // instantiated -- correct, but slower than the fast kernel on B200 so far.
 static int sep_path_mode() {
-    static int mode = -1;
-    if (mode < 0) {
+    static const int mode = [] {  // read once, thread-safe initialisation
         const char* v = std::getenv("IPFC_SEP_PATH");
-        mode = (v && std::strcmp(v, "generic") == 0) ? 1 : (v && std::strcmp(v, "tc") == 0) ? 3 : 0;
-    }
+        return (v && std::strcmp(v, "generic") == 0) ? 1 : (v && std::strcmp(v, "tc") == 0) ? 3 : 0;
+    }();
     return mode;
 }
 
@@ -623,11 +626,10 @@ enum F2DForm { kF2DAuto = 0, kF2DFp32 = 1, kF2DSplit = 2 };
 // with it), the FP32 CUDA-core form otherwise.  IPFC_F2D_PATH=split selects
 // the tensor-core form wherever it applies, =fp32 pins the CUDA-core form.
 static int f2d_auto_form(const ipfc_image* src, const ipfc_image* dst, int kw, int kh) {
-    static int forced = -1;
-    if (forced < 0) {
+    static const int forced = [] {  // read once, thread-safe initialisation
         const char* v = std::getenv("IPFC_F2D_PATH");
-        forced = (v && std::strcmp(v, "fp32") == 0) ? kF2DFp32 : (v && std::strcmp(v, "split") == 0) ? kF2DSplit : 0;
-    }
+        return (v && std::strcmp(v, "fp32") == 0) ? kF2DFp32 : (v && std::strcmp(v, "split") == 0) ? kF2DSplit : 0;
+    }();
     const bool tc_ok = filter2d_tc_eligible(src->dtype, dst->dtype, src->channels, kw, kh);
     if (forced == kF2DSplit && tc_ok) return kF2DSplit;
     if (forced == kF2DFp32) return kF2DFp32;

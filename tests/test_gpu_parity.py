@@ -321,3 +321,43 @@ def test_sep_border_lanes_every_row_residue(gpu, orc, c, dt):
                 G.compare(gpu.sepFilter2D(host, kx, ky, B(b), 0.0, 2.0), want, tol)
                 G.compare(gpu.sepFilter2D(dev, kx, ky, B(b), 0.0, 2.0).cpu().numpy(), want, tol)
                 G.compare(gpu.sepFilter2D(view, kx, ky, B(b), 0.0, 2.0).cpu().numpy(), want, tol)
+
+
+def test_threaded_host_calls_match_single_thread(gpu):
+    """Host-image calls from several threads, each on its own stream (the
+    overlapped form a streaming caller uses), give the single-thread results
+    for every op; each call returns with its result in host memory."""
+    import threading
+
+    import torch
+
+    imgs = [oracle.random_image(300 + 37 * i, 200 + 11 * i, (1, 3, 4)[i % 3], np.uint8, 4242 + i) for i in range(8)]
+    se = gpu.getStructuringElement(gpu.MorphShape.Rect, 3)
+    ops = [lambda im, s: gpu.gaussianBlur(im, 2.0, stream=s),
+           lambda im, s: gpu.gaussianBlur(im, 3.7, border=gpu.BorderMode.Wrap, stream=s),
+           lambda im, s: gpu.medianBlur(im, 5, stream=s),
+           lambda im, s: gpu.erode(im, se, stream=s),
+           lambda im, s: gpu.boxFilter(im, 5, 5, stream=s)]
+    want = [[op(im, None) for op in ops] for im in imgs]
+    got = [[None] * len(ops) for _ in imgs]
+    errors = []
+
+    def worker(k):
+        try:
+            st = torch.cuda.Stream()
+            for rep in range(3):
+                for i in range(k, len(imgs), 4):
+                    for j, op in enumerate(ops):
+                        got[i][j] = op(imgs[i], st)
+        except Exception as e:  # reported below, on the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for i in range(len(imgs)):
+        for j in range(len(ops)):
+            np.testing.assert_array_equal(got[i][j], want[i][j], err_msg=f"image {i} op {j}")
