@@ -166,9 +166,38 @@ void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneV
     const int n = (int)items.size();
     p->items.resize(n);
     std::vector<Tiling> tl(n);
+    std::vector<TuneVal> v(vals.begin(), vals.end());
     for (int i = 0; i < n; ++i) {
         p->items[i] = items[i].it;
-        tl[i] = tile_item(p->items[i], items[i].W, items[i].H, vals[i]);
+        tl[i] = tile_item(p->items[i], items[i].W, items[i].H, v[i]);
+    }
+    // The tuned row counts suit batches of many images.  A separable class
+    // whose tiles fill less than 80 % of its resident CTAs (a few large
+    // images, as a server's batches often are) gets shorter tiles, down to
+    // 2K rows, so that SMs do not idle.
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                   cudaSuccess)
+        cudaGetLastError();
+    const int slots[kBatchClasses] = {2 * sms, sms, 4 * sms};  // resident CTAs per class (registers bound)
+    for (int c : {kBatchLight, kBatchHeavy}) {
+        for (int round = 0; round < 4 && sms > 0; ++round) {
+            long long tiles = 0;
+            for (int i = 0; i < n; ++i)
+                if (tl[i].cls == c && items[i].W > 0 && items[i].H > 0) tiles += (long long)tl[i].nx * tl[i].ny;
+            if (tiles == 0 || 5 * tiles >= 4 * (long long)slots[c]) break;  // at least 80 % of the slots busy
+            bool shrunk = false;
+            for (int i = 0; i < n; ++i) {
+                if (tl[i].cls != c || items[i].it.kind != kBatchSep) continue;
+                const int k = items[i].it.K, rows = std::min(v[i].a, items[i].H);
+                if (rows <= 2 * k) continue;
+                v[i].a = std::max(2 * k, rows / 2);
+                p->items[i] = items[i].it;
+                tl[i] = tile_item(p->items[i], items[i].W, items[i].H, v[i]);
+                shrunk = true;
+            }
+            if (!shrunk) break;
+        }
     }
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
