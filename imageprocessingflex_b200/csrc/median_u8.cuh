@@ -18,8 +18,10 @@
 //    reduced with min/max.u16x2 (two samples per instruction):
 //      k = 3: each window column sorted (3 compare-exchanges), then the
 //             median of (max of minima, median of middles, min of maxima);
-//      k = 5: forgetful selection over the 25 values (keep m + 2 live
-//             values, drop the current minimum and maximum, pull the next);
+//      k = 5: columns then rows sorted, then the 7th smallest of the 13
+//             entries that can still be the median (forgetful selection:
+//             keep m + 2 live values, drop the current minimum and maximum,
+//             pull the next);
 //  * store: one 32-bit store per 4 outputs where the destination address is
 //    4-byte aligned, byte stores otherwise.
 #pragma once
@@ -74,6 +76,26 @@ __device__ __forceinline__ unsigned median9_2(unsigned (&v)[9]) {
     return med3_2(lo, mid, hi);
 }
 
+// Sorts v[i0], v[i0 + st], .. v[i0 + 4 st] ascending (9 compare-exchanges,
+// a minimal 5-input network).
+template <int N>
+__device__ __forceinline__ void sort5_2(unsigned (&v)[N], int i0, int st) {
+    unsigned& a = v[i0];
+    unsigned& b = v[i0 + st];
+    unsigned& c = v[i0 + 2 * st];
+    unsigned& d = v[i0 + 3 * st];
+    unsigned& e = v[i0 + 4 * st];
+    ce2(a, b);
+    ce2(d, e);
+    ce2(c, e);
+    ce2(c, d);
+    ce2(a, d);
+    ce2(a, c);
+    ce2(b, e);
+    ce2(b, d);
+    ce2(b, c);
+}
+
 // Forgetful selection over v[0..N), N = 2m + 1 (see median.cuh).
 template <int N>
 __device__ __forceinline__ unsigned forgetful_2(unsigned (&v)[N]) {
@@ -88,6 +110,22 @@ __device__ __forceinline__ unsigned forgetful_2(unsigned (&v)[N]) {
         v[a + L - 1] = v[u];
     }
     return med3_2(v[m - 1], v[m], v[m + 1]);
+}
+
+// Median of 25 lane-words v[row * 5 + col].  Sort the columns, then the
+// rows: in a matrix sorted both ways the entry at (r, c) has at least
+// (r+1)(c+1) - 1 entries at or below it and (5-r)(5-c) - 1 at or above it,
+// so 6 entries are certainly below the median (rank 13), 6 certainly above,
+// and the median is the 7th smallest of the other 13.  45 + 45 + 45
+// compare-exchanges instead of forgetful selection's 165 over all 25.
+__device__ __forceinline__ unsigned median25_2(unsigned (&v)[25]) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) sort5_2(v, c, 5);  // columns
+#pragma unroll
+    for (int r = 0; r < 5; ++r) sort5_2(v, 5 * r, 1);  // rows
+    unsigned w[13] = {v[3],  v[4],  v[7],  v[8],  v[9],  v[11], v[12],
+                      v[13], v[15], v[16], v[17], v[20], v[21]};
+    return forgetful_2<13>(w);
 }
 
 template <int K>
@@ -164,8 +202,8 @@ __device__ __forceinline__ void median_u8_tile_k(const MedianArgs& a, int TX, in
                 me = median9_2(ev);
                 mo = median9_2(od);
             } else {
-                me = forgetful_2<K * K>(ev);
-                mo = forgetful_2<K * K>(od);
+                me = median25_2(ev);
+                mo = median25_2(od);
             }
             const unsigned acc = lanes_pack(me, mo);
             if (aligned && q + 4 <= rowlen) {
