@@ -66,7 +66,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launches-only", type=int, default=0,
                     help="run this many launches of the workload on one resident image and exit (for ncu captures)")
-    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "serve", "filter2d"],
+    ap.add_argument("--workload", default="headline",
+                    choices=["headline", "batch", "serve", "filter2d", "erode", "median3", "median5"],
                     help="headline: 4K RGB gaussianBlur (the driver's line); batch: 512-image uneven mix, "
                          "batched vs plain per-image launches; serve: Poisson request stream through the "
                          "continuous-batching server vs one request at a time")
@@ -609,8 +610,18 @@ def run_serve(args):
     arms = {}
     for name, kw in (("continuous", {}), ("plain", {"max_inflight": 1, "streams": 1, "batch": False})):
         server = S.Server(**kw)
-        warm = [(i, reqs[i]) for i in range(min(200, len(reqs)))]
-        run_arm(server, [(i, r) for i, r in warm], server.now() - reqs[0].arrival)  # warm-up: all due at once
+        # warm-up, all due at once: the first 200 requests plus the first request
+        # of every (op, taps, channels) kind in the trace, so that every kernel
+        # variant is loaded before the timed replay
+        warm_idx, kinds = list(range(min(200, len(reqs)))), set()
+        for i, r in enumerate(reqs):
+            kind = (r.op, 2 * int(3.0 * r.sigma + 0.5) + 1 if r.op == "gaussian" else 0, r.channels)
+            if kind not in kinds:
+                kinds.add(kind)
+                if i >= 200:
+                    warm_idx.append(i)
+        warm = [(i, reqs[i]) for i in warm_idx]
+        run_arm(server, warm, server.now() - reqs[0].arrival)
         torch.cuda.synchronize()
         t0 = server.now() + 0.1
         with ClockSampler(torch.cuda.current_device()) as clk:
@@ -772,7 +783,9 @@ def launches_only(n, workload="headline"):
       headline -- gaussianBlur(sigma=2) on one 3840x2160x3 uint8 image;
       filter2d -- the split-precision tcgen05 filter2D, 31x31 seeded N(0,1)
                   taps, on one 4096x4096 uint8 image;
-      batch    -- the 512-image uneven mix as one batch (plan, then n runs)."""
+      batch    -- the 512-image uneven mix as one batch (plan, then n runs);
+      erode    -- erode by the 3x3 rectangle on one 3840x2160x3 uint8 image;
+      median3, median5 -- medianBlur 3x3 / 5x5 on that image."""
     import torch
 
     import imageprocessingflex_b200 as ipf
@@ -810,6 +823,11 @@ def launches_only(n, workload="headline"):
         for _ in range(n):
             b.run()
         y = keep[-1]
+    elif workload in ("erode", "median3", "median5"):
+        x = torch.from_numpy(seeded_image(W_IMG, H_IMG, C_IMG)).cuda()
+        se = ipf.getStructuringElement(ipf.MorphShape.Rect, 3)
+        for _ in range(n):
+            y = ipf.erode(x, se) if workload == "erode" else ipf.medianBlur(x, 3 if workload == "median3" else 5)
     else:
         x = torch.from_numpy(seeded_image(W_IMG, H_IMG, C_IMG)).cuda()
         for _ in range(n):
@@ -823,6 +841,10 @@ def main():
     args = parse_args()
     if args.launches_only > 0:
         return launches_only(args.launches_only, args.workload)
+    if args.workload in ("erode", "median3", "median5"):
+        print(f"bench.py: --workload {args.workload} is a profiling program: use it with --launches-only N",
+              file=sys.stderr)
+        return 2
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "batch":
