@@ -144,22 +144,41 @@ __device__ __forceinline__ void morph_u8_tile_impl(const MorphCore& a, int TX, i
         const unsigned* w = reinterpret_cast<const unsigned*>(stage + (size_t)r * g.SP);
         const int dr = delta[r];
         uint2* hr = hrow + (size_t)r * g.TW;
-        for (int t = lane; t < g.TW; t += 32) {
-            const int s0 = 4 * t + dr;
-            const unsigned w0 = staged_word(w, s0);
-            unsigned ev = lanes_even(w0), od = lanes_odd(w0);
-            auto fold_col = [&](int i) {
-                const unsigned wi = staged_word(w, s0 + i * C);
-                ev = fold2<IS_MIN>(ev, lanes_even(wi));
-                od = fold2<IS_MIN>(od, lanes_odd(wi));
-            };
-            if constexpr (SW > 0) {
+        if constexpr (SW > 0) {
+            // window column i of word t starts at byte 4t + dr + i*C: its word
+            // offset and byte selector depend on the row only
+            int off[SW];
+            unsigned sel[SW];
 #pragma unroll
-                for (int i = 1; i < SW; ++i) fold_col(i);
-            } else {
-                for (int i = 1; i < sw; ++i) fold_col(i);
+            for (int i = 0; i < SW; ++i) {
+                const int b = dr + i * C;
+                off[i] = b >> 2;
+                sel[i] = 0x3210u + 0x1111u * (unsigned)(b & 3);
             }
-            hr[t] = make_uint2(ev, od);
+            for (int t = lane; t < g.TW; t += 32) {
+                const unsigned* wt = w + t;
+                const unsigned w0 = __byte_perm(wt[off[0]], wt[off[0] + 1], sel[0]);
+                unsigned ev = lanes_even(w0), od = lanes_odd(w0);
+#pragma unroll
+                for (int i = 1; i < SW; ++i) {
+                    const unsigned wi = __byte_perm(wt[off[i]], wt[off[i] + 1], sel[i]);
+                    ev = fold2<IS_MIN>(ev, lanes_even(wi));
+                    od = fold2<IS_MIN>(od, lanes_odd(wi));
+                }
+                hr[t] = make_uint2(ev, od);
+            }
+        } else {
+            for (int t = lane; t < g.TW; t += 32) {
+                const int s0 = 4 * t + dr;
+                const unsigned w0 = staged_word(w, s0);
+                unsigned ev = lanes_even(w0), od = lanes_odd(w0);
+                for (int i = 1; i < sw; ++i) {
+                    const unsigned wi = staged_word(w, s0 + i * C);
+                    ev = fold2<IS_MIN>(ev, lanes_even(wi));
+                    od = fold2<IS_MIN>(od, lanes_odd(wi));
+                }
+                hr[t] = make_uint2(ev, od);
+            }
         }
     }
     __syncthreads();
