@@ -53,6 +53,16 @@ cudaError_t batch_launch_mem(const BatchItem*, const BatchTile*, int, unsigned*,
 cudaError_t batch_occupancy_light(size_t smem, int* occ);
 cudaError_t batch_occupancy_heavy(size_t smem, int* occ);
 cudaError_t batch_occupancy_mem(size_t smem, int* occ);
+bool batch_sep_group_light(int k, int c, const SepGroup& g, int n, int max_tiles, cudaStream_t s, cudaError_t* e);
+bool batch_sep_group_heavy(int k, int c, const SepGroup& g, int n, int max_tiles, cudaStream_t s, cudaError_t* e);
+
+cudaError_t batch_sep_group_launch(int K, int C, const SepGroup& g, int n, int max_tiles, cudaStream_t s) {
+    cudaError_t e = cudaErrorInvalidValue;
+    if (n < 1 || n > kSepGroupItems || max_tiles < 1) return e;
+    if (batch_sep_group_light(K, C, g, n, max_tiles, s, &e) || batch_sep_group_heavy(K, C, g, n, max_tiles, s, &e))
+        return e;
+    return cudaErrorInvalidValue;
+}
 
 cudaError_t batch_launch(int cls, const BatchItem* items, const BatchTile* tiles, int ntiles, unsigned* counter,
                          int grid, size_t smem, cudaStream_t s) {
@@ -210,8 +220,13 @@ void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneV
         p->tile_off[c] = (int)p->tiles.size();
         p->smem[c] = 0;
         p->cost[c] = 0;
+        p->sep_tiles[c] = 0;
         for (int i : order) {
             if (tl[i].cls != c || items[i].W == 0 || items[i].H == 0) continue;
+            if (items[i].it.kind == kBatchSep) {
+                p->sep_tiles[c] += tl[i].nx * tl[i].ny;
+                continue;  // a group launch (below)
+            }
             p->smem[c] = std::max(p->smem[c], tl[i].smem);
             for (int y = 0; y < tl[i].ny; ++y)
                 for (int x = 0; x < tl[i].nx; ++x) {
@@ -220,6 +235,37 @@ void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneV
                 }
         }
         p->ntiles[c] = (int)p->tiles.size() - p->tile_off[c];
+    }
+    // separable groups: same (K, C), heavy class first, each group's items in
+    // the longest-first order, at most kSepGroupItems per launch
+    p->groups.clear();
+    for (int c : {kBatchHeavy, kBatchLight}) {
+        std::vector<SepGroupLaunch> open;  // the group being filled for each (K, C)
+        for (int i : order) {
+            if (tl[i].cls != c || items[i].it.kind != kBatchSep || items[i].W == 0 || items[i].H == 0) continue;
+            const int K = items[i].it.K, C = items[i].it.C;
+            SepGroupLaunch* gr = nullptr;
+            for (SepGroupLaunch& o : open)
+                if (o.K == K && o.C == C) gr = &o;
+            if (!gr) {
+                open.push_back(SepGroupLaunch{});
+                gr = &open.back();
+                gr->K = K;
+                gr->C = C;
+                gr->cls = c;
+            }
+            gr->items.push_back(i);
+            gr->max_tiles = std::max(gr->max_tiles, tl[i].nx * tl[i].ny);
+            if ((int)gr->items.size() == kSepGroupItems) {
+                p->groups.push_back(*gr);
+                *gr = SepGroupLaunch{};
+                gr->K = K;
+                gr->C = C;
+                gr->cls = c;
+            }
+        }
+        for (const SepGroupLaunch& o : open)
+            if (!o.items.empty()) p->groups.push_back(o);
     }
 }
 
@@ -244,33 +290,47 @@ cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsi
                         cudaEvent_t fork, cudaEvent_t join) {
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * kBatchClasses, s0);
     if (e != cudaSuccess) return e;
-    // Launch order: the heavy class (longest tiles), then the memory-bound
-    // class (its CTAs fit on the SMs beside heavy ones), then the light class.
-    // With side streams each class after the first gets its own branch.
-    const int order[kBatchClasses] = {kBatchHeavy, kBatchMem, kBatchLight};
-    const cudaStream_t lane[kBatchClasses] = {s0, s1, s2};
-    int nonempty = 0;
-    for (int c = 0; c < kBatchClasses; ++c) nonempty += p.ntiles[c] > 0;
-    const bool branches = s1 && s2 && fork && join && nonempty > 1;
-    // the fork follows the counter reset and precedes every launch
-    if (branches && (e = cudaEventRecord(fork, s0)) != cudaSuccess) return e;
-    int used = 0;
-    for (int i = 0; i < kBatchClasses; ++i) {
-        const int c = order[i];
-        if (p.ntiles[c] == 0) continue;
-        cudaStream_t s = s0;
-        if (branches && used > 0) {
-            s = lane[used];
-            if ((e = cudaStreamWaitEvent(s, fork, 0)) != cudaSuccess) return e;
-        }
-        e = batch_launch(c, d_items, d_tiles + p.tile_off[c], p.ntiles[c], d_counter + c, grid[c], p.smem[c], s);
-        if (e != cudaSuccess) return e;
-        ++used;
+    // Three lanes: the heavy separable groups (longest tiles) on s0; the
+    // memory-bound queue on s1 (its CTAs fit on the SMs beside heavy ones);
+    // the light separable groups and the light queue on s2.  Without side
+    // streams everything runs on s0 in that order.
+    bool has_heavy = false, has_light = false;
+    for (const SepGroupLaunch& g : p.groups) (g.cls == kBatchHeavy ? has_heavy : has_light) = true;
+    has_heavy = has_heavy || p.ntiles[kBatchHeavy] > 0;
+    has_light = has_light || p.ntiles[kBatchLight] > 0;
+    const bool has_mem = p.ntiles[kBatchMem] > 0;
+    const bool branches = s1 && s2 && fork && join && (has_heavy + has_mem + has_light) > 1;
+    const cudaStream_t lane_heavy = s0, lane_mem = branches ? s1 : s0, lane_light = branches ? s2 : s0;
+    if (branches) {
+        // the fork follows the counter reset and precedes every launch
+        if ((e = cudaEventRecord(fork, s0)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s1, fork, 0)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s2, fork, 0)) != cudaSuccess) return e;
     }
-    // join: s0 waits for each branch (the event is re-recorded per branch)
-    for (int b = 1; branches && b < used; ++b) {
-        if ((e = cudaEventRecord(join, lane[b])) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(s0, join, 0)) != cudaSuccess) return e;
+    auto run_groups = [&](int cls, cudaStream_t s) -> cudaError_t {
+        SepGroup g{};  // slots past a group's items are never read
+        for (const SepGroupLaunch& gl : p.groups) {
+            if (gl.cls != cls) continue;
+            for (size_t j = 0; j < gl.items.size(); ++j) g.it[j] = p.items[gl.items[j]].u.sep;
+            cudaError_t ge = batch_sep_group_launch(gl.K, gl.C, g, (int)gl.items.size(), gl.max_tiles, s);
+            if (ge != cudaSuccess) return ge;
+        }
+        return cudaSuccess;
+    };
+    auto run_queue = [&](int c, cudaStream_t s) -> cudaError_t {
+        if (p.ntiles[c] == 0) return cudaSuccess;
+        return batch_launch(c, d_items, d_tiles + p.tile_off[c], p.ntiles[c], d_counter + c, grid[c], p.smem[c], s);
+    };
+    if ((e = run_groups(kBatchHeavy, lane_heavy)) != cudaSuccess) return e;
+    if ((e = run_queue(kBatchHeavy, lane_heavy)) != cudaSuccess) return e;
+    if ((e = run_queue(kBatchMem, lane_mem)) != cudaSuccess) return e;
+    if ((e = run_groups(kBatchLight, lane_light)) != cudaSuccess) return e;
+    if ((e = run_queue(kBatchLight, lane_light)) != cudaSuccess) return e;
+    if (branches) {  // join: s0 waits for both branches (the event is re-recorded per branch)
+        for (cudaStream_t s : {s1, s2}) {
+            if ((e = cudaEventRecord(join, s)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(s0, join, 0)) != cudaSuccess) return e;
+        }
     }
     return cudaSuccess;
 }
@@ -684,14 +744,14 @@ int ipfc_batch_info(const ipfc_batch* b, int what, long long* value) {
     switch (what) {
         case IPFC_BATCH_INFO_ITEMS: *value = (long long)b->items.size(); break;
         case IPFC_BATCH_INFO_PLANNED: *value = b->planned ? 1 : 0; break;
-        case IPFC_BATCH_INFO_TILES_LIGHT: *value = p.host.ntiles[kBatchLight]; break;
-        case IPFC_BATCH_INFO_TILES_HEAVY: *value = p.host.ntiles[kBatchHeavy]; break;
+        case IPFC_BATCH_INFO_TILES_LIGHT: *value = p.host.ntiles[kBatchLight] + p.host.sep_tiles[kBatchLight]; break;
+        case IPFC_BATCH_INFO_TILES_HEAVY: *value = p.host.ntiles[kBatchHeavy] + p.host.sep_tiles[kBatchHeavy]; break;
         case IPFC_BATCH_INFO_TILES_MEM: *value = p.host.ntiles[kBatchMem]; break;
         case IPFC_BATCH_INFO_GRID_LIGHT: *value = p.grid[kBatchLight]; break;
         case IPFC_BATCH_INFO_GRID_HEAVY: *value = p.grid[kBatchHeavy]; break;
         case IPFC_BATCH_INFO_GRID_MEM: *value = p.grid[kBatchMem]; break;
-        case IPFC_BATCH_INFO_KERNELS:
-            *value = 0;
+        case IPFC_BATCH_INFO_KERNELS:  // kernel launches per run: queue classes and separable groups
+            *value = (long long)p.host.groups.size();
             for (int c = 0; c < kBatchClasses; ++c) *value += p.host.ntiles[c] > 0;
             break;
         case IPFC_BATCH_INFO_GRAPH: *value = b->exec ? 1 : 0; break;

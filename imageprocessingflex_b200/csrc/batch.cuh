@@ -19,7 +19,9 @@
 // SM; heavy tiles (separable K 15..25) one; memory-bound tiles (3x3 and 5x5
 // median, morphology) at least four, with 64 registers a thread, so that
 // many tiles' loads are in flight and their CTAs fit beside a heavy one.
-// Each class is its own persistent kernel with its own queue.
+// The median and morphology classes are persistent kernels with their own
+// queues; separable tiles run as group launches (below) with the class's
+// CTAs per SM.
 #pragma once
 
 #include "median.cuh"
@@ -57,6 +59,23 @@ struct __align__(16) BatchItem {
         MorphCore morph;
     } u;
 };
+
+// Separable items run as group launches, not from the queues: the argument
+// blocks of up to kSepGroupItems items with the same tap count and channels
+// are the kernel's parameter block, blockIdx.y selects the item and
+// blockIdx.x the tile.  Because the item index comes from blockIdx, the
+// compiler reads the taps and scalars as uniform constant-bank operands, as in
+// the per-image kernel; from the queue's shared-memory copy of the item every
+// use was a load, and a batched tile ran about 1.6x slower than the same tile
+// per image.
+constexpr int kSepGroupItems = 40;  // 40 x 712 B of parameters, within the 32 KB limit
+struct SepGroup {
+    SepFastArgs it[kSepGroupItems];
+};
+
+// Launches a group of n separable uint8 items with K taps and C channels:
+// max_tiles x n CTAs (CTAs past an item's own tiles return at once).
+cudaError_t batch_sep_group_launch(int K, int C, const SepGroup& g, int n, int max_tiles, cudaStream_t s);
 
 // Launches the class-`cls` persistent kernel: `grid` CTAs of kFastThreads
 // threads with `smem` bytes of dynamic shared memory walk tiles[0, ntiles)

@@ -15,10 +15,6 @@ extern __shared__ __align__(128) float g_batch_smem[];
 // Each tile body is its own function: the compiler allocates registers per
 // function, and one kernel body with every variant inlined is many times
 // slower to compile and no faster to run (a call per tile costs nothing).
-template <int K, int C>
-__device__ __noinline__ void batch_sep_tile(int x, int y) {
-    sep_fast_tile<K, C, uint8_t, uint8_t>(g_batch_item.u.sep, g_batch_smem, x, y);
-}
 
 static __device__ __noinline__ void batch_median_tile(int x, int y) {
     median_tile<uint8_t>(g_batch_item.u.med, g_batch_item.tx, g_batch_item.ty, x, y, g_batch_smem);
@@ -35,32 +31,47 @@ static __device__ __noinline__ void batch_morph_tile(int x, int y) {
                   reinterpret_cast<unsigned char*>(g_batch_smem));
 }
 
-// One separable uint8 -> uint8 tile with K taps, channels from the item.
-template <int K>
-__device__ __forceinline__ bool batch_sep_case(int k, int c, int x, int y) {
-    if (k != K) return false;
-    if (c == 1) batch_sep_tile<K, 1>(x, y);
-    else if (c == 3) batch_sep_tile<K, 3>(x, y);
-    else batch_sep_tile<K, 4>(x, y);
-    return true;
-}
-
+// Queue tiles: median k >= 7 (light class), 3x3 / 5x5 median and
+// morphology (memory-bound class).  Separable tiles run as group launches.
 template <int CLS>
 __device__ __forceinline__ void batch_run_tile(int kind, int k, int c, int x, int y) {
     if constexpr (CLS == kBatchLight) {
-        if (kind == kBatchSep) {
-            batch_sep_case<3>(k, c, x, y) || batch_sep_case<5>(k, c, x, y) || batch_sep_case<7>(k, c, x, y) ||
-                batch_sep_case<9>(k, c, x, y) || batch_sep_case<11>(k, c, x, y) || batch_sep_case<13>(k, c, x, y);
-        } else {
-            batch_median_tile(x, y);
-        }
+        batch_median_tile(x, y);
     } else if constexpr (CLS == kBatchMem) {
         if (kind == kBatchMedian) batch_median_u8_tile(x, y);
         else batch_morph_tile(x, y);
-    } else {
-        batch_sep_case<15>(k, c, x, y) || batch_sep_case<17>(k, c, x, y) || batch_sep_case<19>(k, c, x, y) ||
-            batch_sep_case<21>(k, c, x, y) || batch_sep_case<23>(k, c, x, y) || batch_sep_case<25>(k, c, x, y);
     }
+}
+
+// ---- separable group launches --------------------------------------------------
+template <int K, int C>
+__global__ void __launch_bounds__(kFastThreads, K <= kBatchLightMaxTaps ? 2 : 1)
+    batch_sep_group_kernel(const __grid_constant__ SepGroup g) {
+    const SepFastArgs& a = g.it[blockIdx.y];
+    const int chunks = (a.H + a.rows_per_cta - 1) / a.rows_per_cta;
+    if ((int)blockIdx.x >= a.strips * chunks) return;  // CTA-uniform
+    sep_fast_tile<K, C, uint8_t, uint8_t>(a, g_batch_smem, blockIdx.x % a.strips, blockIdx.x / a.strips);
+}
+
+cudaError_t ensure_smem_attr(const void* func, int bytes, unsigned* done_mask);
+
+template <int K, int C>
+cudaError_t batch_sep_group_launch_kc(const SepGroup& g, int n, int max_tiles, cudaStream_t s) {
+    using G = FastGeom<K, C, 4>;
+    static unsigned done = 0;  // one bit per device
+    cudaError_t e = ensure_smem_attr((const void*)batch_sep_group_kernel<K, C>, (int)G::SMEM, &done);
+    if (e != cudaSuccess) return e;
+    batch_sep_group_kernel<K, C><<<dim3(max_tiles, n), kFastThreads, G::SMEM, s>>>(g);
+    return cudaGetLastError();
+}
+
+template <int K>
+bool batch_sep_group_case(int k, int c, const SepGroup& g, int n, int max_tiles, cudaStream_t s, cudaError_t* e) {
+    if (k != K) return false;
+    *e = c == 1   ? batch_sep_group_launch_kc<K, 1>(g, n, max_tiles, s)
+         : c == 3 ? batch_sep_group_launch_kc<K, 3>(g, n, max_tiles, s)
+                  : batch_sep_group_launch_kc<K, 4>(g, n, max_tiles, s);
+    return true;
 }
 
 // The tile loop.  Thread 0 takes the next tile index; the whole CTA reads it

@@ -1,5 +1,6 @@
-// batch_light.cu -- the light-class persistent batch kernel (separable
-// K <= 13, median, morphology) and the separable tile geometry table.
+// batch_light.cu -- the light-class persistent batch kernel (median k >= 7),
+// the separable group launches with K <= 13, and the separable tile geometry
+// table.
 #include "batch_kernel.cuh"
 
 namespace ipfc {
@@ -10,6 +11,14 @@ cudaError_t batch_launch_light(const BatchItem* items, const BatchTile* tiles, i
 }
 
 cudaError_t batch_occupancy_light(size_t smem, int* occ) { return batch_occupancy_class<0>(smem, occ); }
+
+// Separable group launches with K <= 13 taps.
+bool batch_sep_group_light(int k, int c, const SepGroup& g, int n, int max_tiles, cudaStream_t s, cudaError_t* e) {
+    return batch_sep_group_case<3>(k, c, g, n, max_tiles, s, e) || batch_sep_group_case<5>(k, c, g, n, max_tiles, s, e) ||
+           batch_sep_group_case<7>(k, c, g, n, max_tiles, s, e) || batch_sep_group_case<9>(k, c, g, n, max_tiles, s, e) ||
+           batch_sep_group_case<11>(k, c, g, n, max_tiles, s, e) ||
+           batch_sep_group_case<13>(k, c, g, n, max_tiles, s, e);
+}
 
 namespace {
 

@@ -24,13 +24,23 @@ struct HostItem {
 // Items with their tile parameters applied, and the tile list grouped by
 // class (light, heavy, memory-bound), each class ordered by estimated cost
 // per tile.
+// One launch of separable items with the same taps and channels (at most
+// kSepGroupItems): indices into HostPlan::items, and the largest tile count.
+struct SepGroupLaunch {
+    int K = 0, C = 0, cls = 0;
+    int max_tiles = 0;
+    std::vector<int> items;
+};
+
 struct HostPlan {
     std::vector<BatchItem> items;
-    std::vector<BatchTile> tiles;
+    std::vector<BatchTile> tiles;  // queue tiles (median, morphology)
     int ntiles[kBatchClasses] = {};
     int tile_off[kBatchClasses] = {};
     size_t smem[kBatchClasses] = {};
     double cost[kBatchClasses] = {};
+    std::vector<SepGroupLaunch> groups;  // separable items, heavy groups first
+    int sep_tiles[kBatchClasses] = {};  // tiles in the groups, by class
 };
 
 void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneVal>& vals, HostPlan* p);

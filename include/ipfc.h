@@ -224,7 +224,7 @@ enum {
     IPFC_BATCH_INFO_TILES_HEAVY = 3,
     IPFC_BATCH_INFO_GRID_LIGHT = 4,
     IPFC_BATCH_INFO_GRID_HEAVY = 5,
-    IPFC_BATCH_INFO_KERNELS = 6, /* persistent kernel launches per run */
+    IPFC_BATCH_INFO_KERNELS = 6, /* kernel launches per run: queue kernels and separable group launches */
     IPFC_BATCH_INFO_GRAPH = 7,
     IPFC_BATCH_INFO_TILES_MEM = 8, /* 3x3 / 5x5 median and morphology tiles */
     IPFC_BATCH_INFO_GRID_MEM = 9
