@@ -256,6 +256,7 @@ void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneV
             }
             gr->items.push_back(i);
             gr->max_tiles = std::max(gr->max_tiles, tl[i].nx * tl[i].ny);
+            gr->cost += tl[i].cost * tl[i].nx * tl[i].ny;
             if ((int)gr->items.size() == kSepGroupItems) {
                 p->groups.push_back(*gr);
                 *gr = SepGroupLaunch{};
@@ -286,51 +287,71 @@ cudaError_t plan_grids(const HostPlan& p, int grid[kBatchClasses]) {
 }
 
 cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsigned* d_counter, const HostPlan& p,
-                        const int grid[kBatchClasses], cudaStream_t s0, cudaStream_t s1, cudaStream_t s2,
+                        const int grid[kBatchClasses], cudaStream_t s0, const cudaStream_t* side, int nside,
                         cudaEvent_t fork, cudaEvent_t join) {
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * kBatchClasses, s0);
     if (e != cudaSuccess) return e;
-    // Three lanes: the heavy separable groups (longest tiles) on s0; the
-    // memory-bound queue on s1 (its CTAs fit on the SMs beside heavy ones);
-    // the light separable groups and the light queue on s2.  Without side
-    // streams everything runs on s0 in that order.
-    bool has_heavy = false, has_light = false;
-    for (const SepGroupLaunch& g : p.groups) (g.cls == kBatchHeavy ? has_heavy : has_light) = true;
-    has_heavy = has_heavy || p.ntiles[kBatchHeavy] > 0;
-    has_light = has_light || p.ntiles[kBatchLight] > 0;
-    const bool has_mem = p.ntiles[kBatchMem] > 0;
-    const bool branches = s1 && s2 && fork && join && (has_heavy + has_mem + has_light) > 1;
-    const cudaStream_t lane_heavy = s0, lane_mem = branches ? s1 : s0, lane_light = branches ? s2 : s0;
-    if (branches) {
+    // Work units: each separable group launch and each non-empty queue
+    // kernel, with its estimated cost.  Every group launch ends with a tail of
+    // uneven tiles, so with side streams the units are spread over parallel
+    // lanes (largest first, each to the least-loaded lane) and the tails of
+    // one launch overlap the work of others.  Without side streams the units
+    // run on s0: heavy groups, the memory-bound queue, light groups, the
+    // light queue.
+    struct Unit {
+        int group;  // index into p.groups, or -1 - class for a queue kernel
+        double cost;
+    };
+    std::vector<Unit> units;
+    for (int cls : {kBatchHeavy, kBatchLight}) {
+        for (size_t g = 0; g < p.groups.size(); ++g)
+            if (p.groups[g].cls == cls) units.push_back(Unit{(int)g, p.groups[g].cost});
+        if (cls == kBatchHeavy) {
+            for (int c : {kBatchHeavy, kBatchMem})
+                if (p.ntiles[c] > 0) units.push_back(Unit{-1 - c, p.cost[c]});
+        }
+    }
+    if (p.ntiles[kBatchLight] > 0) units.push_back(Unit{-1 - kBatchLight, p.cost[kBatchLight]});
+    const int nl = (side && nside > 0 && fork && join && units.size() > 1)
+                       ? 1 + std::min(nside, (int)units.size() - 1)
+                       : 1;
+    std::vector<cudaStream_t> lane(nl, s0);
+    for (int l = 1; l < nl; ++l) lane[l] = side[l - 1];
+    std::vector<int> of(units.size(), 0);
+    if (nl > 1) {
+        std::vector<size_t> order(units.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t x, size_t y) { return units[x].cost > units[y].cost; });
+        std::vector<double> load(nl, 0.0);
+        for (size_t i : order) {
+            int best = 0;
+            for (int l = 1; l < nl; ++l)
+                if (load[l] < load[best]) best = l;
+            of[i] = best;
+            load[best] += units[i].cost;
+        }
         // the fork follows the counter reset and precedes every launch
         if ((e = cudaEventRecord(fork, s0)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(s1, fork, 0)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(s2, fork, 0)) != cudaSuccess) return e;
+        for (int l = 1; l < nl; ++l)
+            if ((e = cudaStreamWaitEvent(lane[l], fork, 0)) != cudaSuccess) return e;
     }
-    auto run_groups = [&](int cls, cudaStream_t s) -> cudaError_t {
-        SepGroup g{};  // slots past a group's items are never read
-        for (const SepGroupLaunch& gl : p.groups) {
-            if (gl.cls != cls) continue;
+    SepGroup g{};  // slots past a group's items are never read
+    for (size_t i = 0; i < units.size(); ++i) {
+        cudaStream_t s = lane[of[i]];
+        if (units[i].group >= 0) {
+            const SepGroupLaunch& gl = p.groups[units[i].group];
             for (size_t j = 0; j < gl.items.size(); ++j) g.it[j] = p.items[gl.items[j]].u.sep;
-            cudaError_t ge = batch_sep_group_launch(gl.K, gl.C, g, (int)gl.items.size(), gl.max_tiles, s);
-            if (ge != cudaSuccess) return ge;
+            e = batch_sep_group_launch(gl.K, gl.C, g, (int)gl.items.size(), gl.max_tiles, s);
+        } else {
+            const int c = -1 - units[i].group;
+            e = batch_launch(c, d_items, d_tiles + p.tile_off[c], p.ntiles[c], d_counter + c, grid[c], p.smem[c], s);
         }
-        return cudaSuccess;
-    };
-    auto run_queue = [&](int c, cudaStream_t s) -> cudaError_t {
-        if (p.ntiles[c] == 0) return cudaSuccess;
-        return batch_launch(c, d_items, d_tiles + p.tile_off[c], p.ntiles[c], d_counter + c, grid[c], p.smem[c], s);
-    };
-    if ((e = run_groups(kBatchHeavy, lane_heavy)) != cudaSuccess) return e;
-    if ((e = run_queue(kBatchHeavy, lane_heavy)) != cudaSuccess) return e;
-    if ((e = run_queue(kBatchMem, lane_mem)) != cudaSuccess) return e;
-    if ((e = run_groups(kBatchLight, lane_light)) != cudaSuccess) return e;
-    if ((e = run_queue(kBatchLight, lane_light)) != cudaSuccess) return e;
-    if (branches) {  // join: s0 waits for both branches (the event is re-recorded per branch)
-        for (cudaStream_t s : {s1, s2}) {
-            if ((e = cudaEventRecord(join, s)) != cudaSuccess) return e;
-            if ((e = cudaStreamWaitEvent(s0, join, 0)) != cudaSuccess) return e;
-        }
+        if (e != cudaSuccess) return e;
+    }
+    for (int l = 1; l < nl; ++l) {  // join: s0 waits for each lane (the event is re-recorded per lane)
+        if ((e = cudaEventRecord(join, lane[l])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s0, join, 0)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
@@ -367,9 +388,9 @@ cudaError_t make_plan(const std::vector<HostItem>& items, const std::vector<Tune
 
 // Enqueues one execution of a plan: counter reset, then the classes' kernels
 // (on s0, or as parallel branches when s1, s2 and the events are given).
-cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, cudaStream_t s1, cudaStream_t s2, cudaEvent_t fork,
+cudaError_t enqueue_plan(const Plan& p, cudaStream_t s0, const cudaStream_t* side, int nside, cudaEvent_t fork,
                          cudaEvent_t join) {
-    return launch_plan(p.d_items, p.d_tiles, p.d_counter, p.host, p.grid, s0, s1, s2, fork, join);
+    return launch_plan(p.d_items, p.d_tiles, p.d_counter, p.host, p.grid, s0, side, nside, fork, join);
 }
 
 // Times candidate tile shapes for one key on synthetic images; returns the
@@ -442,7 +463,7 @@ cudaError_t tune_key(const TuneKey& key, const HostItem& proto, TuneVal* best) {
         float ms = 1e30f;
         for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
             e = cudaEventRecord(t0, s);
-            if (e == cudaSuccess) e = enqueue_plan(p, s, nullptr, nullptr, nullptr, nullptr);
+            if (e == cudaSuccess) e = enqueue_plan(p, s, nullptr, 0, nullptr, nullptr);
             if (e == cudaSuccess) e = cudaEventRecord(t1, s);
             if (e == cudaSuccess) e = cudaEventSynchronize(t1);
             float m = 0;
@@ -480,7 +501,8 @@ struct ipfc_batch {
     int device = -1;
     bool planned = false;
     Plan plan;
-    cudaStream_t st[3] = {nullptr, nullptr, nullptr};  // capture stream and two branches
+    static constexpr int kLanes = 8;
+    cudaStream_t st[kLanes] = {};  // capture stream and the branches
     cudaEvent_t ev[2] = {nullptr, nullptr};            // fork, join
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -495,7 +517,7 @@ struct ipfc_batch {
     }
     ~ipfc_batch() {
         drop_plan();
-        for (int i = 0; i < 3; ++i)
+        for (int i = 0; i < kLanes; ++i)
             if (st[i]) cudaStreamDestroy(st[i]);
         for (int i = 0; i < 2; ++i)
             if (ev[i]) cudaEventDestroy(ev[i]);
@@ -588,14 +610,14 @@ int plan_batch(ipfc_batch* b, const char* fn) {
     }
     e = make_plan(b->items, vals, &b->plan);
     if (e != cudaSuccess) return cuda_status(e, fn);
-    for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+    for (int i = 0; i < ipfc_batch::kLanes && e == cudaSuccess; ++i)
         if (!b->st[i]) e = cudaStreamCreateWithFlags(&b->st[i], cudaStreamNonBlocking);
     for (int i = 0; i < 2 && e == cudaSuccess; ++i)
         if (!b->ev[i]) e = cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming);
     if (e == cudaSuccess && b->use_graph) {
         e = cudaStreamBeginCapture(b->st[0], cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            cudaError_t e2 = enqueue_plan(b->plan, b->st[0], b->st[1], b->st[2], b->ev[0], b->ev[1]);
+            cudaError_t e2 = enqueue_plan(b->plan, b->st[0], b->st + 1, ipfc_batch::kLanes - 1, b->ev[0], b->ev[1]);
             e = cudaStreamEndCapture(b->st[0], &b->graph);
             if (e2 != cudaSuccess) e = e2;
         }
@@ -733,7 +755,7 @@ int ipfc_batch_run(ipfc_batch* b, void* stream) {
     if (b->exec) {
         e = cudaGraphLaunch(b->exec, s);
     } else {
-        e = enqueue_plan(b->plan, s, nullptr, nullptr, nullptr, nullptr);
+        e = enqueue_plan(b->plan, s, nullptr, 0, nullptr, nullptr);
     }
     return e == cudaSuccess ? IPFC_OK : cuda_status(e, fn);
 }

@@ -29,6 +29,7 @@ struct HostItem {
 struct SepGroupLaunch {
     int K = 0, C = 0, cls = 0;
     int max_tiles = 0;
+    double cost = 0;  // estimated work (sum of its tiles' costs)
     std::vector<int> items;
 };
 
@@ -50,10 +51,11 @@ void build_host_plan(const std::vector<HostItem>& items, const std::vector<TuneV
 cudaError_t plan_grids(const HostPlan& p, int grid[kBatchClasses]);
 
 // Enqueues the plan whose items and tiles are in device memory: resets the
-// class counters, then launches the classes on s0 (or as parallel branches
-// on s0, s1 and s2 when the side streams, fork and join are all given).
+// class counters, then issues the separable group launches and the queue
+// kernels, on s0 in order, or, when nside side streams, fork and join are
+// given, spread over s0 and the side streams as parallel graph branches.
 cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsigned* d_counter, const HostPlan& p,
-                        const int grid[kBatchClasses], cudaStream_t s0, cudaStream_t s1, cudaStream_t s2,
+                        const int grid[kBatchClasses], cudaStream_t s0, const cudaStream_t* side, int nside,
                         cudaEvent_t fork, cudaEvent_t join);
 
 // Tile parameters for an item: the autotuner's entry for its key on the

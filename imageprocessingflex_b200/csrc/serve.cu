@@ -301,7 +301,7 @@ void dispatch_group(ipfc_server* s, Group& g, cudaStream_t st) {
                                 cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
             e = launch_plan((const BatchItem*)dplan, (const BatchTile*)((char*)dplan + ib),
-                            (unsigned*)((char*)dplan + ib + tb), p, grid, st, nullptr, nullptr, nullptr, nullptr);
+                            (unsigned*)((char*)dplan + ib + tb), p, grid, st, nullptr, 0, nullptr, nullptr);
         if (dplan) cudaFreeAsync(dplan, st);
         for (int i : idx) {
             done[i] = 1;
