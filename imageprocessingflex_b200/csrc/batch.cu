@@ -333,11 +333,11 @@ cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsi
         }
         // the fork follows the counter reset and precedes every launch
         if ((e = cudaEventRecord(fork, s0)) != cudaSuccess) return e;
-        for (int l = 1; l < nl; ++l)
-            if ((e = cudaStreamWaitEvent(lane[l], fork, 0)) != cudaSuccess) return e;
     }
+    int forked = 1;  // lanes that wait on the fork; lane 0 is s0 itself
+    while (forked < nl && (e = cudaStreamWaitEvent(lane[forked], fork, 0)) == cudaSuccess) ++forked;
     SepGroup g{};  // slots past a group's items are never read
-    for (size_t i = 0; i < units.size(); ++i) {
+    for (size_t i = 0; i < units.size() && e == cudaSuccess; ++i) {
         cudaStream_t s = lane[of[i]];
         if (units[i].group >= 0) {
             const SepGroupLaunch& gl = p.groups[units[i].group];
@@ -347,13 +347,16 @@ cudaError_t launch_plan(const BatchItem* d_items, const BatchTile* d_tiles, unsi
             const int c = -1 - units[i].group;
             e = batch_launch(c, d_items, d_tiles + p.tile_off[c], p.ntiles[c], d_counter + c, grid[c], p.smem[c], s);
         }
-        if (e != cudaSuccess) return e;
     }
-    for (int l = 1; l < nl; ++l) {  // join: s0 waits for each lane (the event is re-recorded per lane)
-        if ((e = cudaEventRecord(join, lane[l])) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(s0, join, 0)) != cudaSuccess) return e;
+    // Join every forked lane, after an error too, so that a stream capture
+    // in progress ends with all its branches merged back into s0: s0 waits
+    // for each lane (the event is re-recorded per lane).
+    for (int l = 1; l < forked; ++l) {
+        cudaError_t j = cudaEventRecord(join, lane[l]);
+        if (j == cudaSuccess) j = cudaStreamWaitEvent(s0, join, 0);
+        if (e == cudaSuccess) e = j;
     }
-    return cudaSuccess;
+    return e;
 }
 
 TuneVal tuned_or_default(int kind, int k, int c, int W, int H) {
