@@ -72,6 +72,8 @@ constexpr int kSepGroupItems = 40;  // 40 x 712 B of parameters, within the 32 K
 struct SepGroup {
     SepFastArgs it[kSepGroupItems];
 };
+// The whole group is one kernel's parameter block, whose limit is 32764 bytes.
+static_assert(sizeof(SepGroup) <= 32764, "a separable group must fit in the kernel parameters");
 
 // Launches a group of n separable uint8 items with K taps and C channels:
 // max_tiles x n CTAs (CTAs past an item's own tiles return at once).
