@@ -1,4 +1,4 @@
-"""Batches: many device images through one persistent launch (ipfc_batch_*).
+"""Batches: many device images through a few launches (ipfc_batch_*).
 
 A ``Batch`` collects per-image calls -- ``add_gaussianBlur``,
 ``add_sepFilter2D``, ``add_medianBlur``, ``add_erode``, ``add_dilate``, with

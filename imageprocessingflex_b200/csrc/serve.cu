@@ -269,7 +269,8 @@ void dispatch_group(ipfc_server* s, Group& g, cudaStream_t st) {
         if (e != cudaSuccess) q.status = cuda_status(e, "server");
         e = cudaSuccess;
     }
-    // kernels: the batchable requests as one persistent launch
+    // kernels: the batchable requests as one batch plan (separable group
+    // launches and persistent queue kernels)
     std::vector<HostItem> items;
     std::vector<TuneVal> vals;
     std::vector<int> idx;

@@ -6,9 +6,9 @@ tensors for host images, CUDA tensors for device images) and the op's
 parameters -- with an arrival time on the server's clock; the server's
 scheduler thread admits requests against its slot and device-memory budget,
 overlaps them over several streams and merges those the batch kernels cover
-into one persistent launch.  ``poll`` returns completions with their arrival,
-admission and completion times.  The caller keeps every image alive and
-unchanged until its request completes.
+into one batch plan for each group of requests admitted together.  ``poll``
+returns completions with their arrival, admission and completion times.  The
+caller keeps every image alive and unchanged until its request completes.
 """
 from __future__ import annotations
 

@@ -191,16 +191,19 @@ IPFC_API int ipfc_erode(const ipfc_image* src, ipfc_image* dst, const uint8_t* s
 IPFC_API int ipfc_dilate(const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w, int se_h, int iterations,
                 void* stream);
 
-/* ---- batches: many images, one persistent launch -------------------------
+/* ---- batches: many images, a few launches --------------------------------
  *
  * No counterpart in the reference (ipf runs one call per image).  A batch
  * collects per-image calls -- the same functions and arguments as the
  * entry points above, on device images -- and runs them together: every
- * image is cut into the per-image kernels' tiles, and persistent kernels
- * walk one tile queue over all images.  The first ipfc_batch_run plans the
- * batch (autotuned tile shapes, tile order, device tables) and captures it
- * as a CUDA graph; later runs replay the graph on `stream`.  Each image's
- * result is bit-identical to its per-image call.
+ * image is cut into the per-image kernels' tiles.  Separable items with the
+ * same taps and channels share one launch (up to 40 items, their arguments
+ * in the kernel parameters); median and morphology tiles are walked by
+ * persistent kernels, one tile queue per register class, over all images.
+ * The launches are spread over parallel graph branches.  The first
+ * ipfc_batch_run plans the batch (autotuned tile shapes, tile order, device
+ * tables) and captures it as a CUDA graph; later runs replay the graph on
+ * `stream`.  Each image's result is bit-identical to its per-image call.
  *
  * Covered: uint8 images with 1, 3 or 4 channels; separable filters and
  * gaussianBlur with equal odd tap counts 3..25 and centred anchors;

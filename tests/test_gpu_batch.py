@@ -1,5 +1,5 @@
-"""The batched form (ipfc_batch_*): persistent kernels walking one tile queue
-over many uneven uint8 images, replayed as a CUDA graph.
+"""The batched form (ipfc_batch_*): separable group launches and persistent
+tile-queue kernels over many uneven uint8 images, replayed as a CUDA graph.
 
 The tile bodies are the per-image kernels' own code, so every batched image
 must equal its per-image call bit for bit; the per-image calls are held to
