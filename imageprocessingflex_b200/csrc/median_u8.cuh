@@ -52,18 +52,18 @@ __host__ __device__ inline size_t median_u8_tile_bytes(int TX, int TY, int k, in
     return MedianU8Geom(TX, TY, k, C).bytes();
 }
 
-__device__ __forceinline__ void ce2(unsigned& a, unsigned& b) {
+__host__ __device__ __forceinline__ void ce2(unsigned& a, unsigned& b) {
     const unsigned lo = umin2(a, b), hi = umax2(a, b);
     a = lo;
     b = hi;
 }
 
-__device__ __forceinline__ unsigned med3_2(unsigned a, unsigned b, unsigned c) {
+__host__ __device__ __forceinline__ unsigned med3_2(unsigned a, unsigned b, unsigned c) {
     return umax2(umin2(a, b), umin2(umax2(a, b), c));
 }
 
 // median of 9 lane-words: v[dy * 3 + dx]
-__device__ __forceinline__ unsigned median9_2(unsigned (&v)[9]) {
+__host__ __device__ __forceinline__ unsigned median9_2(unsigned (&v)[9]) {
 #pragma unroll
     for (int dx = 0; dx < 3; ++dx) {  // sort each column
         ce2(v[dx], v[3 + dx]);
@@ -79,7 +79,7 @@ __device__ __forceinline__ unsigned median9_2(unsigned (&v)[9]) {
 // Sorts v[i0], v[i0 + st], .. v[i0 + 4 st] ascending (9 compare-exchanges,
 // a minimal 5-input network).
 template <int N>
-__device__ __forceinline__ void sort5_2(unsigned (&v)[N], int i0, int st) {
+__host__ __device__ __forceinline__ void sort5_2(unsigned (&v)[N], int i0, int st) {
     unsigned& a = v[i0];
     unsigned& b = v[i0 + st];
     unsigned& c = v[i0 + 2 * st];
@@ -98,7 +98,7 @@ __device__ __forceinline__ void sort5_2(unsigned (&v)[N], int i0, int st) {
 
 // Forgetful selection over v[0..N), N = 2m + 1 (see median.cuh).
 template <int N>
-__device__ __forceinline__ unsigned forgetful_2(unsigned (&v)[N]) {
+__host__ __device__ __forceinline__ unsigned forgetful_2(unsigned (&v)[N]) {
     constexpr int m = N / 2;
 #pragma unroll
     for (int round = 0; round < m - 1; ++round) {
@@ -118,7 +118,7 @@ __device__ __forceinline__ unsigned forgetful_2(unsigned (&v)[N]) {
 // so 6 entries are certainly below the median (rank 13), 6 certainly above,
 // and the median is the 7th smallest of the other 13.  45 + 45 + 45
 // compare-exchanges instead of forgetful selection's 165 over all 25.
-__device__ __forceinline__ unsigned median25_2(unsigned (&v)[25]) {
+__host__ __device__ __forceinline__ unsigned median25_2(unsigned (&v)[25]) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) sort5_2(v, c, 5);  // columns
 #pragma unroll

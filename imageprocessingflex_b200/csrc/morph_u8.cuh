@@ -33,16 +33,29 @@ namespace ipfc {
 
 constexpr int kMorphU8Threads = 256;
 
-// 16-bit lane min / max (two lanes per instruction)
-__device__ __forceinline__ unsigned umin2(unsigned a, unsigned b) {
+// 16-bit lane min / max (two lanes per instruction).  The host form, lane
+// by lane, lets host programs run the selection networks built on these.
+__host__ __device__ __forceinline__ unsigned umin2(unsigned a, unsigned b) {
+#ifdef __CUDA_ARCH__
     unsigned r;
     asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
     return r;
+#else
+    const unsigned lo = (a & 0xffffu) < (b & 0xffffu) ? (a & 0xffffu) : (b & 0xffffu);
+    const unsigned hi = (a >> 16) < (b >> 16) ? (a >> 16) : (b >> 16);
+    return (hi << 16) | lo;
+#endif
 }
-__device__ __forceinline__ unsigned umax2(unsigned a, unsigned b) {
+__host__ __device__ __forceinline__ unsigned umax2(unsigned a, unsigned b) {
+#ifdef __CUDA_ARCH__
     unsigned r;
     asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
     return r;
+#else
+    const unsigned lo = (a & 0xffffu) > (b & 0xffffu) ? (a & 0xffffu) : (b & 0xffffu);
+    const unsigned hi = (a >> 16) > (b >> 16) ? (a >> 16) : (b >> 16);
+    return (hi << 16) | lo;
+#endif
 }
 // bytes (b0, b1, b2, b3) -> lanes (b0, b2) and (b1, b3), and back
 __device__ __forceinline__ unsigned lanes_even(unsigned w) { return __byte_perm(w, 0u, 0x4240u); }
