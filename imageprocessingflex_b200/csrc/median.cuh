@@ -23,7 +23,7 @@ namespace ipfc {
 
 namespace median_detail {
 
-__device__ __forceinline__ float med3(float a, float b, float c) {
+__host__ __device__ __forceinline__ float med3(float a, float b, float c) {
     return fmaxf(fminf(a, b), fminf(fmaxf(a, b), c));
 }
 
@@ -31,7 +31,7 @@ __device__ __forceinline__ float med3(float a, float b, float c) {
 // unseen value v[u].  Each round bubbles the live minimum to v[a] and the live
 // maximum to v[a+L-1], drops both, and moves v[u] into the freed maximum slot.
 template <int N>
-__device__ __forceinline__ float median_forgetful(float (&v)[N]) {
+__host__ __device__ __forceinline__ float median_forgetful(float (&v)[N]) {
     constexpr int m = N / 2;
 #pragma unroll
     for (int round = 0; round < m - 1; ++round) {

@@ -1,11 +1,14 @@
-"""The packed uint8 median networks of the 3x3 and 5x5 median kernels
-(median9_2, median25_2 in csrc/median_u8.cuh), proven exact on the host.
+"""The median selection networks of the 3x3 and 5x5 median kernels, proven
+exact on the host: the packed uint8 networks (median9_2, median25_2 in
+csrc/median_u8.cuh) and the forgetful selection of the other element types
+(median_forgetful in csrc/median.cuh).
 
-median_network_check.cu compiles the kernels' own header for the host and
-runs both networks on every binary window (2^9 and 2^25 of them).  The
+median_network_check.cu compiles the kernels' own headers for the host and
+runs each network on every binary window (2^9 and 2^25 of them).  The
 networks use only min and max, so by the 0-1 principle that covers every
-uint8 window; a sample of random byte windows checks the two-lane packing
-against std::nth_element as well.  medianBlur's reference result is the
+window of ordered values (uint8; uint16, int16 and non-NaN floats for the
+forgetful selection); a sample of random byte windows checks the two-lane
+packing against std::nth_element as well.  medianBlur's reference result is the
 sample of rank k*k/2 of the window (include/ipf/filter.hpp:302-332).
 """
 import os
@@ -37,4 +40,4 @@ def test_median_networks_exact_on_every_binary_window(tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([out], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.strip() == f"ok {(1 << 9) + (1 << 25) + 400000}", r.stdout
+    assert r.stdout.strip() == f"ok {2 * ((1 << 9) + (1 << 25)) + 400000}", r.stdout
