@@ -84,7 +84,7 @@ cudaError_t prepare_device() {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const unsigned bit = 1u << (dev & 31);
+    const unsigned bit = dev >= 0 && dev < 32 ? 1u << dev : 0u;  // devices past 32 are set up every call
     if (__atomic_load_n(&g_pool_ready, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
     cudaMemPool_t pool;
     e = cudaDeviceGetDefaultMemPool(&pool, dev);
@@ -112,8 +112,11 @@ unsigned* device_error_word() {
         cudaGetLastError();
         return nullptr;
     }
+    // Past the table no word is kept: the kernels skip the error write when
+    // given none, and ipfc_check_device then reports nothing.
+    if (dev < 0 || dev >= 32) return nullptr;
     std::lock_guard<std::mutex> lk(g_err_word_mu);
-    unsigned*& w = g_err_word[dev & 31];
+    unsigned*& w = g_err_word[dev];
     if (!w) {
         unsigned* p = nullptr;
         if (cudaMalloc((void**)&p, sizeof(unsigned)) != cudaSuccess ||

@@ -287,7 +287,7 @@ cudaError_t ensure_smem_attr(const void* func, int bytes, unsigned* done_mask) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const unsigned bit = 1u << (dev & 31);
+    const unsigned bit = dev >= 0 && dev < 32 ? 1u << dev : 0u;  // devices past 32 are set every call
     if (__atomic_load_n(done_mask, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
     e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) __atomic_fetch_or(done_mask, bit, __ATOMIC_ACQ_REL);
