@@ -92,10 +92,13 @@ typedef struct ipfc_image {
 
 /* ---- library ------------------------------------------------------------- */
 
-/* Thread-local text of the last failure on this thread ("" when none). */
+/* Thread-local text of the last failure on this thread ("" when none).
+ * Replaces the message of ipf::Error (include/ipf/core.hpp:35-41): argument
+ * errors carry the same "ipf: <function>: <reason>" text. */
 IPFC_API const char* ipfc_last_error(void);
 
-/* (major << 16) | (minor << 8) | patch of this library. */
+/* (major << 16) | (minor << 8) | patch of this library (its own numbering,
+ * not IPF_VERSION_* of include/ipf/core.hpp:24-26). */
 IPFC_API int ipfc_version(void);
 
 /* Waits for `stream`, then reports whether any kernel since the last check
