@@ -103,13 +103,13 @@ __device__ __forceinline__ float to_f(T v) {
 
 // Round half away from zero.  truncf() is exact; the remainder x - t is exact
 // for |x| < 2^24 and for larger |x| it is 0, so no rounding step is involved.
-__device__ __forceinline__ float round_half_away(float x) {
+__host__ __device__ __forceinline__ float round_half_away(float x) {
     const float t = truncf(x);
     return fabsf(x - t) >= 0.5f ? t + copysignf(1.0f, x) : t;
 }
 
 template <typename T>
-__device__ __forceinline__ T sat_from_f(float v) {
+__host__ __device__ __forceinline__ T sat_from_f(float v) {
     if constexpr (Elem<T>::is_int) {
         // fmaxf/fminf return the non-NaN operand, so NaN lands on lo or hi:
         // pin NaN to 0 explicitly as the reference does.
