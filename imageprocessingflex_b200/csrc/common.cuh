@@ -62,7 +62,7 @@ __host__ __device__ __forceinline__ int floor_div(int a, int b) {
 
 // Resolves a flat interleaved sample index s = x*C + c of a row of `width`
 // pixels to the flat index of its border source, or -1 (Constant outside).
-__device__ __forceinline__ int border_sample(int s, int width, int C, int mode) {
+__host__ __device__ __forceinline__ int border_sample(int s, int width, int C, int mode) {
     const int x = floor_div(s, C);
     const int c = s - x * C;
     const int sx = border_index(x, width, mode);

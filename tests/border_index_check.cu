@@ -5,7 +5,11 @@
 //
 //  * every row length 1..256 and every position from -4n - 40 to 5n + 40;
 //  * sampled lengths up to the C ABI's limit (2^30 - 1 samples per row),
-//    with positions around both row ends and a full kernel halo away.
+//    with positions around both row ends and a full kernel halo away;
+//  * the interleaved form the tile loaders use (border_sample: sample
+//    index x*C + c to its source sample, channel kept) for C = 1..4, every
+//    row length 1..128 and every sample from a few rows left to a few rows
+//    right of the row.
 //
 // Prints "ok <cases checked>" and exits 0, or prints the first failures and
 // exits 1.
@@ -42,6 +46,17 @@ int main() {
             }
         }
     }
+    for (int mode = 0; mode < 5; ++mode)
+        for (int C = 1; C <= 4; ++C)
+            for (int w = 1; w <= 128; ++w)
+                for (int s = -(4 * w + 10) * C; s < (5 * w + 10) * C; ++s) {
+                    const int x = s >= 0 ? s / C : -((-s + C - 1) / C), c = s - x * C;
+                    const int sx = orc_border_index(x, w, mode);
+                    const int want = sx < 0 ? -1 : sx * C + c, got = ipfc::border_sample(s, w, C, mode);
+                    ++checked;
+                    if (got != want && bad++ < 5)
+                        std::printf("sample: mode %d C %d w %d s %d: %d, oracle %d\n", mode, C, w, s, got, want);
+                }
     if (bad) {
         std::printf("FAILED %lld of %lld\n", bad, checked);
         return 1;

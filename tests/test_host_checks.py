@@ -6,7 +6,8 @@ the oracle's C restatement:
 * border_index_check.cu: the border rule (border_index) against borderIndex
   (include/ipf/core.hpp:187-214) on every position of every row length up
   to 256 and on sampled lengths up to the C ABI's limit of 2^30 - 1 samples
-  per row, for all five border modes;
+  per row, for all five border modes, and its interleaved form
+  (border_sample) for 1 to 4 channels;
 * saturate_check.cu: the store rounding (sat_from_f) against saturate_cast
   (include/ipf/core.hpp:69-103) on all 2^32 float bit patterns, to uint8,
   uint16 and int16.
