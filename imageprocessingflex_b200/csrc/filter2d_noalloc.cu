@@ -10,14 +10,23 @@
 // file-scope device array below (kNoAllocMaxTaps entries, 64 KB, held by
 // every GPU that loads the library until the process exits), and nothing is
 // allocated per call.  The caller passes device images only (host images
-// would need staging buffers).
+// would need staging buffers).  It always runs the FP32 CUDA-core form, the
+// same kernel as ipfc_filter2d_fp32 (ipfc_filter2d may pick the tensor-core
+// form for single-channel uint8 images from 15 x 15 taps, whose uint8
+// results can differ from this one by 1 LSB; both stay within 1 LSB of ipf).
 //
 // Set-up: the first call on each device looks up the array's device address
-// with cudaGetSymbolAddress while that device is current, so that first call
-// should come before any stream capture.  The array is shared by every call
-// and keeps the last call's taps: two calls whose kernels overlap on the GPU
-// (on different streams) race on it.  Each call writes exactly the entries
-// its kernel reads, so nothing has to start at zero.
+// with cudaGetSymbolAddress while that device is current.  The taps travel
+// from a per-thread pageable host buffer with cudaMemcpyAsync, which a
+// capturing stream refuses, and a captured copy would replay the buffer's
+// contents at replay time; so a call on a capturing stream is rejected with
+// IPFC_ERR_UNSUPPORTED before anything is enqueued.  The array is shared by
+// every call and keeps the last call's taps: any two calls whose streams the
+// caller has not ordered (by using the same stream, an event or a
+// synchronisation) race on it, even when their kernels would not run at the
+// same time, because the second call's copy may land before the first call's
+// kernel starts.  Each call writes exactly the entries its kernel reads, so
+// nothing has to start at zero.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -40,6 +49,8 @@ constexpr int kNoAllocMaxTaps = 4096;  // 64 KB of {w, dx, dy, 0}
 // address: kernels get the address looked up below.
 static __device__ __align__(256) float4 g_noalloc_taps[kNoAllocMaxTaps];
 
+// Per-device address of the array; threads may race to fill an entry, and
+// every racer stores the same value, so acquire/release atomics suffice.
 float4* g_taps_addr[32] = {nullptr};
 
 // Device address of g_noalloc_taps on the current device (looked up once).
@@ -47,14 +58,17 @@ int taps_address(float4** out, const char* fn) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return ipfc::cuda_status(e, fn);
-    if (dev >= 32) return ipfc::set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: device index %d out of range", fn, dev);
-    if (!g_taps_addr[dev]) {
+    if (dev < 0 || dev >= 32)
+        return ipfc::set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: device index %d out of range", fn, dev);
+    float4* addr = __atomic_load_n(&g_taps_addr[dev], __ATOMIC_ACQUIRE);
+    if (!addr) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_taps);
         if (e != cudaSuccess) return ipfc::cuda_status(e, fn);
-        g_taps_addr[dev] = static_cast<float4*>(p);
+        addr = static_cast<float4*>(p);
+        __atomic_store_n(&g_taps_addr[dev], addr, __ATOMIC_RELEASE);
     }
-    *out = g_taps_addr[dev];
+    *out = addr;
     return IPFC_OK;
 }
 
@@ -101,10 +115,18 @@ extern "C" IPFC_API int ipfc_filter2d_noalloc(const ipfc_image* src, ipfc_image*
     if (src->width == 0 || src->height == 0) return IPFC_OK;
     if (!src->data || !dst->data) return set_error(IPFC_ERR_INVALID, "ipf: %s: null pixel pointer", fn);
     if (src->data == dst->data) return set_error(IPFC_ERR_INVALID, "ipf: %s: in-place operation is not supported", fn);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(s, &cap);
+    if (ce != cudaSuccess) return cuda_status(ce, fn);
+    if (cap != cudaStreamCaptureStatusNone)
+        return set_error(IPFC_ERR_UNSUPPORTED,
+                         "ipf: %s: cannot be called while its stream is capturing (the taps are copied from a "
+                         "per-thread host buffer)",
+                         fn);
     float4* taps = nullptr;
     int rc = taps_address(&taps, fn);
     if (rc) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
     // Host copy of the list, copied into the static array on the stream.  A
     // copy from pageable memory returns once the source has been read, so
     // this thread may reuse the buffer on its next call.

@@ -151,16 +151,6 @@ IPFC_API int ipfc_sobel(const ipfc_image* src, ipfc_image* dst, int dx, int dy, 
 IPFC_API int ipfc_filter2d(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax, int ay,
                   int border, double delta, double border_value, void* stream);
 
-/* filter2D for callers that cannot allocate device memory (inside a custom
- * allocator, under a framework that reserved the device's memory, in a
- * pipeline that forbids allocation after start-up).  Same result as
- * ipfc_filter2d, device images only; the non-zero taps are staged in a fixed
- * 64 KB device array that the library holds on every GPU it runs on, so at
- * most 4096 non-zero taps (larger kernels are rejected with
- * IPFC_ERR_INVALID).  The first call on a device looks up that array's
- * address (do it before any stream capture).  Calls share the array: calls
- * whose kernels overlap on the GPU race on it.  No counterpart in the
- * reference, whose CPU code allocates freely. */
 /* The two forms of filter2D behind ipfc_filter2d, for callers that choose:
  *  ipfc_filter2d_fp32  -- CUDA cores, FP32 accumulation, every channel count
  *                         and element type;
@@ -178,6 +168,20 @@ IPFC_API int ipfc_filter2d_fp32(const ipfc_image* src, ipfc_image* dst, const fl
 IPFC_API int ipfc_filter2d_split(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax,
                                  int ay, int border, double delta, double border_value, void* stream);
 
+/* filter2D for callers that cannot allocate device memory (inside a custom
+ * allocator, under a framework that reserved the device's memory, in a
+ * pipeline that forbids allocation after start-up).  It always runs the FP32
+ * CUDA-core form, the same kernel and result as ipfc_filter2d_fp32 (not
+ * necessarily ipfc_filter2d's, which may pick the tensor-core form), on
+ * device images only.  The non-zero taps are staged in a fixed 64 KB device
+ * array that the library holds on every GPU it runs on, so at most 4096
+ * non-zero taps (larger kernels are rejected with IPFC_ERR_INVALID).  The
+ * first call on a device looks up that array's address.  A call on a
+ * capturing stream is rejected with IPFC_ERR_UNSUPPORTED: the taps are
+ * copied from a per-thread host buffer.  Calls share the array: any two calls
+ * whose streams the caller has not ordered (same stream, an event or a
+ * synchronisation) race on it.  No counterpart in the reference, whose CPU
+ * code allocates freely. */
 IPFC_API int ipfc_filter2d_noalloc(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax,
                                    int ay, int border, double delta, double border_value, void* stream);
 
