@@ -145,6 +145,37 @@ class CpuFilters:
             raise ValueError(f"ipf: filter2D failed ({rc})")
         return out
 
+    def filter2d_rows(self, src, kernel, y0, y1, border=REFLECT101, delta=0.0, anchor=(-1, -1), border_value=0.0,
+                      out_dtype=None, threads=0):
+        """Output rows [y0, y1) of filter2D over the whole image (restatement
+        only), computed by ``threads`` host threads (0: all cores) on
+        sub-bands; the C routine runs without the GIL."""
+        import concurrent.futures as cf
+
+        src = np.ascontiguousarray(src)
+        k = np.ascontiguousarray(kernel, np.float32)
+        kh, kw = k.shape
+        W, H, C = _shape(src)
+        y0, y1 = max(0, y0), min(H, y1)
+        shape = (y1 - y0,) + src.shape[1:]
+        out = np.zeros(shape, np.dtype(out_dtype) if out_dtype is not None else src.dtype)
+        f = self._f("filter2d_rows")
+        nt = threads or os.cpu_count() or 1
+        step = max(1, -(-(y1 - y0) // nt))
+        row_bytes = out[0].nbytes if out.shape[0] else 0
+
+        def band(a):
+            b = min(y1, a + step)
+            dst = ctypes.c_void_p(out.ctypes.data + (a - y0) * row_bytes)
+            return f(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, dst, DTYPE_CODE[out.dtype], _ptr(k), kw, kh,
+                     anchor[0], anchor[1], border, _c_double(delta), _c_double(border_value), a, b)
+
+        with cf.ThreadPoolExecutor(nt) as ex:
+            rcs = list(ex.map(band, range(y0, y1, step)))
+        if any(rcs):
+            raise ValueError(f"ipf: filter2D failed ({rcs})")
+        return out
+
     def box_filter(self, src, kw, kh, normalize=True, border=REFLECT101, border_value=0.0, out_dtype=None):
         src = np.ascontiguousarray(src)
         out = self._out(src, out_dtype)

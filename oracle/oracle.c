@@ -10,7 +10,7 @@
  * floating-point operation order (FP64 accumulation, same summation order, no
  * FMA contraction: build with -ffp-contract=off), so that its results are
  * bit-identical to the reference's for the same inputs.  Parity is pinned two
- * ways (tests/test_oracle_*.py): against the reference's own known-answer
+ * ways (tests/test_oracle.py): against the reference's own known-answer
  * tests (tests/test_filter.cpp, tests/test_morphology.cpp) and against the
  * reference headers compiled into oracle/_ref/ on many seeded inputs.
  *
@@ -279,9 +279,22 @@ int orc_sep_filter(const void* src, int sdt, int W, int H, int C, void* dst, int
  * taps are dropped; each sample starts at delta and adds the remaining taps in
  * row-major order in FP64, then saturates.
  * ------------------------------------------------------------------------- */
+/* Output rows [y0, y1) of filter2D over the whole image; dst holds only those
+ * rows (y1 - y0 rows of W*C samples).  Lets a test check full-width bands of
+ * a large image -- its top, bottom and interior -- without the whole image. */
+int orc_filter2d_rows(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, const float* kernel, int kw,
+                      int kh, int ax, int ay, int border, double delta, double border_value, int y0, int y1);
+
 int orc_filter2d(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, const float* kernel, int kw, int kh,
                  int ax, int ay, int border, double delta, double border_value) {
+    return orc_filter2d_rows(src, sdt, W, H, C, dst, ddt, kernel, kw, kh, ax, ay, border, delta, border_value, 0, H);
+}
+
+int orc_filter2d_rows(const void* src, int sdt, int W, int H, int C, void* dst, int ddt, const float* kernel, int kw,
+                      int kh, int ax, int ay, int border, double delta, double border_value, int y0, int y1) {
     if (kw <= 0 || kh <= 0) return ORC_EINVAL;
+    if (y0 < 0) y0 = 0;
+    if (y1 > H) y1 = H;
     if (ax < 0) ax = kw / 2;
     if (ay < 0) ay = kh / 2;
     if (ax >= kw || ay >= kh) return ORC_EINVAL;
@@ -306,7 +319,7 @@ int orc_filter2d(const void* src, int sdt, int W, int H, int C, void* dst, int d
                 ++ntap;
             }
         }
-    for (int y = 0; y < H; ++y)
+    for (int y = y0; y < y1; ++y)
         for (int x = 0; x < W; ++x)
             for (int c = 0; c < C; ++c) {
                 double s = delta;
@@ -315,7 +328,7 @@ int orc_filter2d(const void* src, int sdt, int W, int H, int C, void* dst, int d
                     s += tw[t] * ((sx < 0 || sy < 0) ? border_value
                                                      : load_elem(src, sdt, ((size_t)sy * W + sx) * C + c));
                 }
-                store_sat(dst, ddt, ((size_t)y * W + x) * C + c, s);
+                store_sat(dst, ddt, ((size_t)(y - y0) * W + x) * C + c, s);
             }
     free(tdx); free(tdy); free(tw); free(xt); free(yt);
     return ORC_OK;

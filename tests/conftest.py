@@ -41,3 +41,16 @@ def gpu():
     import imageprocessingflex_b200 as ipf
 
     return ipf
+
+
+def pytest_terminal_summary(terminalreporter):
+    """Where the parity bar was wider than 1 LSB / 1e-5, and by how much."""
+    try:
+        import golden_cases
+    except ImportError:
+        return
+    lines = golden_cases.widened_report()
+    if lines:
+        terminalreporter.write_sep("-", "parity cases on a widened bar (FP32 summation bound above 1 LSB / 1e-5)")
+        for ln in lines:
+            terminalreporter.write_line(ln)

@@ -129,7 +129,7 @@ def fp32_bound(op, p, x):
 
 
 def tolerance(op, p, x, want):
-    """(kind, value, bound) of the parity bar for a GPU result against the reference.
+    """(kind, value, bound, op) of the parity bar for a GPU result against the reference.
 
     exact  -- integer arithmetic: median, morphology, box on integer sources,
               Sobel and other integer-tap separable filters on integer sources
@@ -154,12 +154,36 @@ def tolerance(op, p, x, want):
                 return ("exact", 0, 0.0)
     bound = fp32_bound(op, p, x)
     if want.dtype.kind in "iu":
-        return ("lsb", max(1, int(np.ceil(bound + 0.5))), bound)
-    return ("rel", 1e-5, bound)
+        return ("lsb", max(1, int(np.ceil(bound + 0.5))), bound, op)
+    return ("rel", 1e-5, bound, op)
+
+
+# Cases whose bar is wider than the headline one (1 LSB for integer outputs,
+# 1e-5 x max(1, |ref|) for float outputs): op -> [count, widest bar, largest
+# observed error].  conftest.py prints it at the end of the run, so the suite
+# shows where and by how much the bar was relaxed.
+WIDENED = {}
+
+
+def _note_widened(op, kind, bar, observed):
+    w = WIDENED.setdefault((op, kind), [0, 0.0, 0.0])
+    w[0] += 1
+    w[1] = max(w[1], float(bar))
+    w[2] = max(w[2], float(observed))
+
+
+def widened_report():
+    lines = []
+    for (op, kind), (n, bar, obs) in sorted(WIDENED.items()):
+        unit = "LSB" if kind == "lsb" else "abs"
+        lines.append(f"{op:10s} {kind:4s} {n:5d} cases above the 1 LSB / 1e-5 bar: widest bar {bar:.3g} {unit}, "
+                     f"largest observed error {obs:.3g} {unit}")
+    return lines
 
 
 def compare(got, want, tol):
-    kind, v, bound = tol
+    kind, v, bound = tol[:3]
+    op = tol[3] if len(tol) > 3 else "?"
     assert got.shape == want.shape and got.dtype == want.dtype, (got.shape, got.dtype, want.shape, want.dtype)
     if kind == "exact":
         bad = np.flatnonzero(got != want)
@@ -168,8 +192,13 @@ def compare(got, want, tol):
         return 0
     d = np.abs(got.astype(np.float64) - want.astype(np.float64))
     if kind == "lsb":
+        if v > 1:
+            _note_widened(op, kind, v, d.max(initial=0))
         assert d.max(initial=0) <= v, f"max |diff| {d.max()} > {v} LSB"
         return int((d > 0).sum())
-    lim = np.maximum(v * np.maximum(1.0, np.abs(want.astype(np.float64))), bound)
+    base = v * np.maximum(1.0, np.abs(want.astype(np.float64)))
+    lim = np.maximum(base, bound)
+    if d.size and bound > base.min():
+        _note_widened(op, kind, bound, d.max())
     assert np.all(d <= lim), f"max |diff| {d.max()} exceeds max({v} x max(1, |ref|), FP32 bound {bound:.3g})"
     return 0
