@@ -48,10 +48,8 @@ bool make_sep_fast_args(const ipfc_image* src, const ipfc_image* dst, const void
                         void* out_ptr, long long out_pitch, const double* kx, int kw, const double* ky, int kh, int ax,
                         int ay, int border, double delta, double bv, SepFastArgs* fp);
 cudaError_t batch_launch_light(const BatchItem*, const BatchTile*, int, unsigned*, int, size_t, cudaStream_t);
-cudaError_t batch_launch_heavy(const BatchItem*, const BatchTile*, int, unsigned*, int, size_t, cudaStream_t);
 cudaError_t batch_launch_mem(const BatchItem*, const BatchTile*, int, unsigned*, int, size_t, cudaStream_t);
 cudaError_t batch_occupancy_light(size_t smem, int* occ);
-cudaError_t batch_occupancy_heavy(size_t smem, int* occ);
 cudaError_t batch_occupancy_mem(size_t smem, int* occ);
 bool batch_sep_group_light(int k, int c, const SepGroup& g, int n, int max_tiles, cudaStream_t s, cudaError_t* e);
 bool batch_sep_group_heavy(int k, int c, const SepGroup& g, int n, int max_tiles, cudaStream_t s, cudaError_t* e);
@@ -66,15 +64,16 @@ cudaError_t batch_sep_group_launch(int K, int C, const SepGroup& g, int n, int m
 
 cudaError_t batch_launch(int cls, const BatchItem* items, const BatchTile* tiles, int ntiles, unsigned* counter,
                          int grid, size_t smem, cudaStream_t s) {
+    // the heavy class has no queue tiles (its separable items are group launches)
     if (cls == kBatchLight) return batch_launch_light(items, tiles, ntiles, counter, grid, smem, s);
-    if (cls == kBatchHeavy) return batch_launch_heavy(items, tiles, ntiles, counter, grid, smem, s);
-    return batch_launch_mem(items, tiles, ntiles, counter, grid, smem, s);
+    if (cls == kBatchMem) return batch_launch_mem(items, tiles, ntiles, counter, grid, smem, s);
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t batch_occupancy(int cls, size_t smem, int* occ) {
     if (cls == kBatchLight) return batch_occupancy_light(smem, occ);
-    if (cls == kBatchHeavy) return batch_occupancy_heavy(smem, occ);
-    return batch_occupancy_mem(smem, occ);
+    if (cls == kBatchMem) return batch_occupancy_mem(smem, occ);
+    return cudaErrorInvalidValue;
 }
 
 namespace {

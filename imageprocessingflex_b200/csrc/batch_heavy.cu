@@ -1,15 +1,8 @@
-// batch_heavy.cu -- the separable group launches with 15 to 25 taps (and
-// the heavy class's persistent kernel, which no queue tile uses now).
+// batch_heavy.cu -- the separable group launches with 15 to 25 taps.  The
+// heavy class holds only group launches: no queue tile belongs to it.
 #include "batch_kernel.cuh"
 
 namespace ipfc {
-
-cudaError_t batch_launch_heavy(const BatchItem* items, const BatchTile* tiles, int ntiles, unsigned* counter, int grid,
-                               size_t smem, cudaStream_t s) {
-    return batch_launch_class<1>(items, tiles, ntiles, counter, grid, smem, s);
-}
-
-cudaError_t batch_occupancy_heavy(size_t smem, int* occ) { return batch_occupancy_class<1>(smem, occ); }
 
 // Separable group launches with 15 to 25 taps.
 bool batch_sep_group_heavy(int k, int c, const SepGroup& g, int n, int max_tiles, cudaStream_t s, cudaError_t* e) {

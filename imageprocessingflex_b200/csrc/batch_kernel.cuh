@@ -77,7 +77,7 @@ bool batch_sep_group_case(int k, int c, const SepGroup& g, int n, int max_tiles,
 // The tile loop.  Thread 0 takes the next tile index; the whole CTA reads it
 // after a barrier, so every exit and item switch is CTA-uniform.
 template <int CLS>
-__global__ void __launch_bounds__(kFastThreads, CLS == kBatchLight ? 2 : CLS == kBatchHeavy ? 1 : 4)
+__global__ void __launch_bounds__(kFastThreads, CLS == kBatchLight ? 2 : 4)
     batch_kernel(const BatchItem* __restrict__ items, const BatchTile* __restrict__ tiles, int ntiles,
                  unsigned* __restrict__ counter) {
     __shared__ int next;

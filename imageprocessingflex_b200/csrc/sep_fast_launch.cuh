@@ -18,13 +18,16 @@ cudaError_t launch_sep_fast(const SepFastArgs& in, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     int dev = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    // Resident CTAs per SM, cached per device (devices past the table are
+    // queried every call).  Racing threads store the same value.
     static int occ_cache[32] = {0};
-    int occ = occ_cache[dev & 31];
+    const bool cached = dev >= 0 && dev < 32;
+    int occ = cached ? __atomic_load_n(&occ_cache[dev], __ATOMIC_ACQUIRE) : 0;
     if (occ == 0) {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFastThreads, G::SMEM);
         if (e != cudaSuccess) return e;
         occ = occ > 0 ? occ : 1;
-        occ_cache[dev & 31] = occ;
+        if (cached) __atomic_store_n(&occ_cache[dev], occ, __ATOMIC_RELEASE);
     }
     int sms = 0;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;

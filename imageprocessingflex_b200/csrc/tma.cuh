@@ -1,4 +1,4 @@
-// tma.cuh -- mbarrier and TMA (cp.async.bulk.tensor) helpers, sm_100a.
+// tma.cuh -- mbarrier helpers (bounded waits) for the tcgen05 kernels, sm_100a.
 //
 // Every wait is bounded: try_wait spins at most kSpinLimit times; on expiry
 // the caller's error word gets the given code (first writer wins) and the
@@ -13,12 +13,8 @@
 namespace ipfc {
 
 // About 2^24 polls (tens of milliseconds): far above any legitimate wait
-// for a TMA row load, short enough to bound a stuck kernel.
+// for a stage of a tensor-core pipeline, short enough to bound a stuck kernel.
 constexpr unsigned kSpinLimit = 1u << 24;
-
-// Error codes written to the device error word.
-constexpr unsigned kErrWaitFull = 0x101u;   // a TMA row never arrived
-constexpr unsigned kErrWaitEmpty = 0x102u;  // consumers never released a stage
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -68,29 +64,5 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsign
     if (err) atomicCAS(err, 0u, code);
     return false;
 }
-
-// 2-D tiled TMA load of the map's box at element coordinates {x, y} into
-// shared memory, completing its bytes on the mbarrier.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// L2 prefetch of the same box (no shared-memory destination).
-__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
-    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
-                 "r"(x), "r"(y)
-                 : "memory");
-}
-
-// Host: encodes a 2-D tensor map over rows of 32-bit words (row_bytes / 4
-// words, `rows` rows, `pitch` bytes apart) with a box of {box_words, 1}.
-// Returns false when the layout does not meet TMA's rules (16-byte aligned
-// base and pitch, whole words per row) or the driver call fails.
-bool encode_row_map_u32(CUtensorMap* map, const void* base, long long row_bytes, int rows, long long pitch,
-                        int box_words);
 
 }  // namespace ipfc

@@ -273,9 +273,10 @@ def test_tc_separable_path(gpu):
 @pytest.mark.parametrize("c", [1, 3, 4])
 @pytest.mark.parametrize("w", [1200, 1201])
 def test_medium_all_borders_u8(gpu, orc, c, w):
-    """Images wide enough for interior strips: the TMA row ring (w*c a
-    multiple of 4) and the load path (otherwise), every border, host arrays
-    and device tensors, against the restatement within 1 LSB."""
+    """Images wide enough for interior strips: aligned rows (w*c a multiple
+    of 4, one word load per lane) and unaligned rows (border-lane word
+    copies), every border, host arrays and device tensors, against the
+    restatement within 1 LSB."""
     import torch
 
     img = oracle.random_image(w, 157, c, np.uint8, 7 * c + w)
