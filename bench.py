@@ -65,6 +65,9 @@ def parse_args():
                     help="host threads (each with its own stream) calling the synchronous C ABI in the e2e leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave the shortened filter2D / batch / serve measurements out of the default line")
+    ap.add_argument("--extras-serve-requests", type=int, default=3000)
     ap.add_argument("--launches-only", type=int, default=0,
                     help="run this many launches of the workload on one resident image and exit (for ncu captures)")
     ap.add_argument("--workload", default="headline",
@@ -376,6 +379,8 @@ def run_ours(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = time_cpu_baseline(host, args.cpu_seconds)
+        if world == 1 and not args.no_extras:
+            line.update(measure_extras(args))
         print(json.dumps(line), flush=True)
     del graph
     if world > 1:
@@ -383,7 +388,54 @@ def run_ours(args):
     return 0
 
 
-def run_batch(args):
+def measure_extras(args):
+    """The other measured configurations, shortened, for the default line:
+    split vs FP32 filter2D 31x31 on 4096x4096 uint8 (with FP64 error), the
+    512-image batched uneven mix against per-image launches, and a served
+    stream of `extras_serve_requests` requests (continuous vs one at a time).
+    Each is the same code as its --workload line, with fewer steps."""
+    out = {}
+    t0 = time.perf_counter()
+    try:
+        rows, tf, _, _ = filter2d_cases(args, (("u8", 31),), 5)
+        r = tf[("u8", 31)]
+        out["d3_filter2d_31x31_u8_4096"] = {
+            "split_ms": r["split"]["ms"], "fp32_ms": r["fp32"]["ms"], "speedup_split_vs_fp32": r["speedup_split_vs_fp32"],
+            "split_tflops": r["split"]["tflops"], "split_frac_of_bf16_peak": r["split"]["frac_of_bf16_peak"],
+            "fp32_frac_of_fp32_fma_peak": r["fp32"]["frac_of_fp32_fma_peak"],
+            "err_vs_fp64_max": {"split": r["split"]["err_vs_fp64_max"], "fp32": r["fp32"]["err_vs_fp64_max"]},
+            "err_vs_fp64_mean": {"split": r["split"]["err_vs_fp64_mean"], "fp32": r["fp32"]["err_vs_fp64_mean"]},
+            "u8_max_lsb": r["split"].get("u8_max_lsb"), "u8_mismatch_rate": r["split"].get("u8_mismatch_rate"),
+            "error_sample": "1024x512 crop, same taps"}
+    except Exception as exc:  # reported, never silently dropped
+        out["d3_filter2d_31x31_u8_4096"] = {"error": str(exc)[:300]}
+    try:
+        ba = argparse.Namespace(**vars(args))
+        ba.steps, ba.warmup = 5, 2
+        bl = run_batch(ba, quiet=True)
+        out["d4_batch_512"] = {"batched_ms": bl["batched"]["ms"], "plain_ms": bl["plain"]["ms"],
+                               "speedup_vs_plain": bl["speedup_vs_plain"], "mpix_s": bl["value"],
+                               "results_equal_per_image": bl["results_equal_per_image"],
+                               "roofline_frac": bl["roofline"]["frac"], "kernels_per_step": bl["gpu_launches"] // 5,
+                               "plan_seconds": bl["batched"]["plan_seconds"]}
+    except Exception as exc:
+        out["d4_batch_512"] = {"error": str(exc)[:300]}
+    try:
+        sa = argparse.Namespace(**vars(args))
+        sa.serve_requests = args.extras_serve_requests
+        sl = run_serve(sa, quiet=True)
+        c, p = sl["continuous"], sl["plain"]
+        out["d5_serve"] = {"requests": sa.serve_requests, "rate_per_s": sa.serve_rate,
+                           "continuous": {k: c[k] for k in ("p50_ms", "p99_ms", "mpix_s", "failed")},
+                           "plain": {k: p[k] for k in ("p50_ms", "p99_ms", "mpix_s", "failed")},
+                           "speedup_vs_plain_mpix": sl["speedup_vs_plain_mpix"]}
+    except Exception as exc:
+        out["d5_serve"] = {"error": str(exc)[:300]}
+    out["extras_seconds"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
+def run_batch(args, quiet=False):
     """The batched uneven mix (512 uint8 images, w and h uniform in [64, 2048],
     channels from {1, 3, 4}; gaussianBlur sigma ~ U[0.5, 4] 50 %, medianBlur 3
     or 5 25 %, erode / dilate 3x3 rect 25 %), resident in HBM.  Three forms of
@@ -481,7 +533,7 @@ def run_batch(args):
     # where the per-image form's time goes: each op's images alone
     by_op = {}
     all_items, all_views = items, views
-    for op in ("gaussian", "median", "erode", "dilate"):
+    for op in (() if quiet else ("gaussian", "median", "erode", "dilate")):
         sel = [i for i, it in enumerate(all_items) if it.op == op]
         items = [all_items[i] for i in sel]
         views = [all_views[i] for i in sel]
@@ -522,12 +574,14 @@ def run_batch(args):
                      "alg_bytes_per_step": int(alg_bytes)},
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
     b.close()
+    if quiet:
+        return line
+    print(json.dumps(line), flush=True)
     return 0
 
 
-def run_serve(args):
+def run_serve(args, quiet=False):
     """The served stream: `serve_requests` requests with Poisson arrivals at
     `serve_rate`/s (area lognormal, median 1 MP, log-sd 1, clipped to
     0.01-33 MP; aspect U[0.5, 2]; C in {1, 3}; uint8; gaussianBlur 45 %,
@@ -663,6 +717,8 @@ def run_serve(args):
         "e2e": {"value": c["mpix_s"], "unit": UNIT, "h2d_bytes_per_step": in_total, "d2h_bytes_per_step": out_total},
         "clocks": c["clocks"],
     }
+    if quiet:
+        return line
     print(json.dumps(line), flush=True)
     return 0
 
@@ -675,6 +731,30 @@ def run_filter2d(args):
     than L2 are not needed: the op is compute-bound; two image pairs rotate).
     Errors against the FP64 oracle are measured on a 1024x512 crop of the same
     kind of image with the same taps."""
+    results, tf, tc_peak, tc_peak_source = filter2d_cases(args, (("u8", 15), ("u8", 31), ("f32", 15), ("f32", 31)),
+                                                          args.steps)
+    head = tf[("u8", 31)]
+    line = {
+        "metric": METRIC, "value": head["split"]["mpix_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["split"]["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8 pixels exact in f16, taps f16 hi+lo, f32 accumulate",
+        "data": "synthetic (seeded uniform)",
+        "config": {"workload": "filter2D 4096x4096x1, dense N(0,1) taps normalised to sum 1, Reflect101; FP32 "
+                               "CUDA-core form vs split-precision tcgen05 form", "value_is": "u8 31x31 split Mpix/s",
+                   "flops_per_launch": "2*W*H*kw*kh (counted once, not per hi/lo product)"},
+        "cases": results,
+        "roofline": {"bound": "tensor", "achieved": head["split"]["tflops"], "peak": tc_peak, "unit": "TFLOP/s",
+                     "frac": head["split"]["frac_of_bf16_peak"], "traffic": None,
+                     "peak_source": tc_peak_source},
+        "gpu_launches": (args.steps + args.warmup) * 8,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def filter2d_cases(args, cases, steps):
+    """Times the FP32 and split forms of filter2D on 4096x4096x1 for each
+    (dtype, k) of `cases`; returns (rows, rows by case, tensor peak, its source)."""
     import numpy as np
     import torch
 
@@ -701,6 +781,8 @@ def run_filter2d(args):
     orc = oracle.restatement()
     results = []
     for dt in ("u8", "f32"):
+        if not any(c[0] == dt for c in cases):
+            continue
         g = torch.Generator(device=dev)
         g.manual_seed(3)
         if dt == "u8":
@@ -716,6 +798,8 @@ def run_filter2d(args):
                  for x, y in zip(srcs, dsts)]
         crop = oracle.random_image(1024, 512, 1, np.uint8 if dt == "u8" else np.float32, 11)
         for kk in (15, 31):
+            if (dt, kk) not in cases:
+                continue
             taps = mix.filter2d_taps(kk, seed=1000 + kk)
             tp = taps.ctypes.data
             row = {"dtype": dt, "taps": f"{kk}x{kk}"}
@@ -725,17 +809,17 @@ def run_filter2d(args):
                     rc = fn(ctypes.byref(sv), ctypes.byref(dv), tp, kk, kk, -1, -1, BORDER_REFLECT101, 0.0, 0.0, sptr)
                     if rc:
                         raise RuntimeError(lib.ipfc_last_error().decode())
-                steps = max(2, args.steps if form == "split" else min(args.steps, 5))
+                nsteps = max(2, steps if form == "split" else min(steps, 5))
                 for i in range(args.warmup):
                     step(i)
                 stream.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                for i in range(steps):
+                for i in range(nsteps):
                     step(i)
                 e1.record(stream)
                 e1.synchronize()
-                ms = e0.elapsed_time(e1) / steps
+                ms = e0.elapsed_time(e1) / nsteps
                 flops = 2.0 * N * N * kk * kk
                 row[form] = {"ms": round(ms, 4), "mpix_s": round(N * N / (ms / 1e3) / 1e6, 1),
                              "tflops": round(flops / (ms / 1e3) / 1e12, 2)}
@@ -758,23 +842,7 @@ def run_filter2d(args):
                 row["saturated_fraction"] = float(f"{((want == 0) | (want == 255)).mean():.4g}")
             results.append(row)
             tf[(dt, kk)] = row
-    head = tf[("u8", 31)]
-    line = {
-        "metric": METRIC, "value": head["split"]["mpix_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": head["split"]["ms"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8 pixels exact in f16, taps f16 hi+lo, f32 accumulate",
-        "data": "synthetic (seeded uniform)",
-        "config": {"workload": "filter2D 4096x4096x1, dense N(0,1) taps normalised to sum 1, Reflect101; FP32 "
-                               "CUDA-core form vs split-precision tcgen05 form", "value_is": "u8 31x31 split Mpix/s",
-                   "flops_per_launch": "2*W*H*kw*kh (counted once, not per hi/lo product)"},
-        "cases": results,
-        "roofline": {"bound": "tensor", "achieved": head["split"]["tflops"], "peak": tc_peak, "unit": "TFLOP/s",
-                     "frac": head["split"]["frac_of_bf16_peak"], "traffic": None,
-                     "peak_source": tc_peak_source},
-        "gpu_launches": (args.steps + args.warmup) * 8,
-    }
-    print(json.dumps(line), flush=True)
-    return 0
+    return results, tf, tc_peak, tc_peak_source
 
 
 def run_sep_sweep(args):

@@ -1,0 +1,503 @@
+// sep_tcol.cu -- separable correlation of uint8 images (sepFilter2D,
+// gaussianBlur, include/ipf/filter.hpp:37-90, 197-203, 262-267) with the
+// column pass on tcgen05 tensor cores and the row pass on CUDA cores reading
+// tensor memory directly.  Geometry and the GEMM form: sep_tcol.cuh.
+//
+// One persistent CTA per SM walks its share of (band, slab) units (128
+// output rows x 128 interleaved samples), runs of one band bracketed by halo
+// steps (TcolWalk).  Warp roles:
+//  * warp 0: allocates 512 tensor-memory columns (four slab buffers); its
+//    lane 0 issues, per step, KR/16 K steps x (A_hi, A_lo) MMAs into the
+//    step's buffer and commits them to the B-empty and T-full barriers;
+//  * warps 1-4 (producers): per step, load the band's KR source rows of the
+//    slab (16-byte loads; rows and samples outside the image resolved by the
+//    border mode, Constant as the border value), convert uint8 - 128 to FP16
+//    exactly (byte permutes into 0x64xx, minus 1152) and store them into one
+//    of two B buffers;
+//  * warps 5-12 (row pass): warp w reads tensor-memory lanes 32 (w mod 4) ..
+//    +31 -- one output row per thread -- and half the slab's columns, plus
+//    C*(K/2) columns either side from the neighbouring slab buffers; runs the
+//    K horizontal taps (FP32 FMAs with the taps as constant-bank operands);
+//    rounds with one add toward -inf onto 2^23 (the +0.5 and every constant
+//    term are folded into the accumulator's start value); packs bytes and
+//    stores 16-byte runs of its output row.
+// Handshakes are mbarriers (B full/empty, T full/empty) with bounded waits.
+// A wait that gives up records kErrTcolWait in the device error word and
+// sets an abort flag that every role checks per step.  Tensor memory is
+// freed only after a final commit barrier shows every issued MMA complete;
+// if even that bounded wait gives up, the memory is left allocated rather
+// than freed under a running MMA (kErrTcolDrain).
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "../../include/ipfc.h"
+#include "common.cuh"
+#include "sep_fast.cuh"
+#include "sep_tcol.cuh"
+#include "tc_common.cuh"
+
+namespace ipfc {
+
+unsigned* device_error_word();
+cudaError_t ensure_smem_attr(const void* func, int bytes, unsigned* done_mask);
+
+constexpr unsigned kErrTcolWait = 0x301u;   // a pipeline wait gave up
+constexpr unsigned kErrTcolDrain = 0x302u;  // the final MMA drain gave up: tensor memory left allocated
+
+struct TcolArgs {
+    const unsigned char* src;
+    long long spitch;
+    unsigned char* dst;
+    long long dpitch;
+    int W, H, rowlen;
+    int border;
+    unsigned short bvh;  // FP16 bits of (Constant border value - 128)
+    int nb, ns, units;   // bands, slabs per band, nb * ns
+    int clamp;           // outputs may leave [0, 255]
+    int vec_store;       // destination base and pitch are 16-byte aligned
+    float off;           // 128 * sum(ky) * sum(kx) + delta + 0.5
+    unsigned long long wait_ns;   // a pipeline wait gives up after this long
+    unsigned short ahi[kTcolMaxK + 1], alo[kTcolMaxK + 1];  // FP16 bits of ky * 2^e (hi, lo)
+    float kx[kTcolMaxK + 1];                                 // kx * 2^-e
+    unsigned* err;
+};
+
+namespace {
+
+__device__ __forceinline__ unsigned long long tcol_clock_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait on a barrier phase.  The bound is wall time (a.wait_ns on the
+// global timer), not a poll count: try_wait may suspend the thread for a
+// system-dependent time per poll.  Gives up early when another role has set
+// the abort flag; a wait that runs out records kErrTcolWait and sets it.
+__device__ __forceinline__ bool tcol_wait(uint64_t* bar, unsigned parity, const TcolArgs& a, volatile int* abort_flag) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = tcol_clock_ns();
+    for (unsigned i = 1;; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 63u) == 0) {
+            if (*abort_flag) return false;
+            if (tcol_clock_ns() - t0 > a.wait_ns) break;
+        }
+    }
+    if (a.err) atomicCAS(a.err, 0u, kErrTcolWait);
+    *abort_flag = 1;
+    return false;
+}
+
+// tcgen05.ld of 16 consecutive columns of this warp's lane quarter; the
+// registers are valid after tcol_ld_wait on the same array.
+__device__ __forceinline__ void tcol_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t* r = reinterpret_cast<uint32_t*>(v);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+// Waits for this thread's outstanding tensor-memory loads; the array is an
+// in/out operand so no use of it moves above the wait.
+__device__ __forceinline__ void tcol_ld_wait(float (&v)[16]) {
+    uint32_t* r = reinterpret_cast<uint32_t*>(v);
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])::"memory");
+}
+
+// uint8 word -> two FP16x2 words of (byte - 128), exact.
+__device__ __forceinline__ void tcol_cvt_word(unsigned w, unsigned& h01, unsigned& h23) {
+    const __half2 k1152 = __halves2half2(__ushort_as_half((unsigned short)0x6480), __ushort_as_half((unsigned short)0x6480));
+    const unsigned u01 = __byte_perm(w, 0x64646464u, 0x4140u);
+    const unsigned u23 = __byte_perm(w, 0x64646464u, 0x4342u);
+    h01 = h2_bits(__hsub2(*reinterpret_cast<const __half2*>(&u01), k1152));
+    h23 = h2_bits(__hsub2(*reinterpret_cast<const __half2*>(&u23), k1152));
+}
+
+// FP16 bits of one border-resolved sample (slow path: edges of the image).
+__device__ __forceinline__ unsigned short tcol_sample_h(const TcolArgs& a, const unsigned char* srow, int g, int C) {
+    const int sx = srow ? border_sample(g, a.W, C, a.border) : -1;
+    if (sx < 0) return a.bvh;
+    return __half_as_ushort(__float2half_rn((float)srow[sx] - 128.f));
+}
+
+}  // namespace
+
+template <int K, int C>
+__global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_constant__ TcolArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    constexpr int KR = tcol_kr(K);
+    constexpr int KSTEPS = KR / 16;
+    constexpr int KG = KR / 8;
+    constexpr int GH = tcol_halo_groups(K, C);  // halo groups of 16 columns either side
+    constexpr int R = C * (K / 2);
+    static_assert(GH <= 2, "row-pass window: at most 32 columns of halo");
+    constexpr int NG = 4 + 2 * GH;  // column groups one row-pass thread reads per step
+
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + tcol_off_bar(K));
+    uint64_t* bfull = bars;        // [2] producers -> MMA
+    uint64_t* bempty = bars + 2;   // [2] MMA commit -> producers
+    uint64_t* tfull = bars + 4;    // [4] MMA commit -> row pass
+    uint64_t* tempty = bars + 8;   // [4] row pass -> MMA
+    uint64_t* drain = bars + 12;   // final commit
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 13);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 14);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_u32(sm);
+
+    // ---- set-up: barriers, tensor memory, the banded tap operands A_hi, A_lo
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&bfull[i], 32 * kTcolProdWarps);
+            mbar_init(&bempty[i], 1);
+        }
+        for (int i = 0; i < 4; ++i) {
+            mbar_init(&tfull[i], 1);
+            mbar_init(&tempty[i], kTcolRowWarps);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, kTcolTmemCols);
+    // A: one 16-byte core-matrix row (fixed m, 8 consecutive k) per item
+    for (int it = tid; it < 2 * kTcolM * KG; it += kTcolThreads) {
+        const int hl = it / (kTcolM * KG), rest = it % (kTcolM * KG);
+        const int m = rest % kTcolM, kg = rest / kTcolM;
+        const unsigned short* tap = hl ? a.alo : a.ahi;
+        unsigned w[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int j0 = 8 * kg + 2 * e - m, j1 = j0 + 1;
+            const unsigned lo = (j0 >= 0 && j0 < K) ? tap[j0] : 0u;
+            const unsigned hi = (j1 >= 0 && j1 < K) ? tap[j1] : 0u;
+            w[e] = lo | (hi << 16);
+        }
+        *reinterpret_cast<uint4*>(sm + tcol_off_a(hl, K) + tcol_a_off(m, 8 * kg)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *tslot;
+
+    const int u0 = (int)((long long)blockIdx.x * a.units / gridDim.x);
+    const int u1 = (int)((long long)(blockIdx.x + 1) * a.units / gridDim.x);
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ MMA issue
+        if (lane == 0) {
+            TcolWalk walk(u0, u1, a.ns);
+            TcolStep st;
+            int g = 0;
+            bool issued = false;
+            const uint32_t a_hi = sbase + tcol_off_a(0, K), a_lo = sbase + tcol_off_a(1, K);
+            while (walk.next(st)) {
+                if (*abort_flag) break;
+                const int bb = g & 1, tb = g & 3;
+                if (!tcol_wait(&bfull[bb], (unsigned)(g >> 1) & 1u, a, abort_flag)) break;
+                if (g >= 4 && !tcol_wait(&tempty[tb], (unsigned)((g - 4) >> 2) & 1u, a, abort_flag)) break;
+                tc_fence_after();
+                const int n0 = st.kind == 2 ? 0 : st.kind == 0 ? kTcolN - 16 * GH : 0;
+                const int nn = st.kind == 1 ? kTcolN : 16 * GH;
+                const uint32_t idesc = tcol_idesc(nn);
+                const uint32_t bsm = sbase + tcol_off_b(bb, K);
+                const uint32_t d = tbase + (uint32_t)(tb * kTcolN + n0);
+#pragma unroll 1
+                for (int ks = 0; ks < KSTEPS; ++ks) {
+                    const uint64_t bd = tcol_desc_b(bsm, ks, n0);
+                    tc_mma(d, tcol_desc_a(a_hi, ks), bd, idesc, ks > 0 ? 1u : 0u);
+                    tc_mma(d, tcol_desc_a(a_lo, ks), bd, idesc, 1u);
+                }
+                tc_commit(&bempty[bb]);
+                tc_commit(&tfull[tb]);
+                issued = true;
+                ++g;
+            }
+            if (issued) tc_commit(drain);
+            // leave the drain barrier's phase complete when nothing was issued
+            else mbar_arrive(drain);
+        }
+        __syncwarp();
+    } else if (warp <= kTcolProdWarps) {
+        // ------------------------------------------------------------ producers
+        const int pw = warp - 1, r8 = lane & 7, c4 = lane >> 3;
+        TcolWalk walk(u0, u1, a.ns);
+        TcolStep st;
+        int g = 0;
+        while (walk.next(st)) {
+            if (*abort_flag) break;
+            const int bb = g & 1;
+            if (g >= 2 && !tcol_wait(&bempty[bb], (unsigned)((g - 2) >> 1) & 1u, a, abort_flag)) break;
+            unsigned char* B = sm + tcol_off_b(bb, K);
+            const int y0 = st.band * kTcolM - K / 2;
+            const int x0 = st.slab * kTcolN;
+            // samples this step needs: the whole slab, or a halo edge
+            const int n_lo = st.kind == 0 ? kTcolN - 16 * GH : 0;
+            const int n_hi = st.kind == 2 ? 16 * GH : kTcolN;
+            // items: (K group, half of the slab); lane = (row in group, 16-sample chunk of the half)
+            constexpr int ITEMS = KG * 2;
+            constexpr int PER = (ITEMS + kTcolProdWarps - 1) / kTcolProdWarps;
+            uint4 raw[PER];
+            bool fast[PER];
+#pragma unroll
+            for (int r = 0; r < PER; ++r) {
+                const int it = pw + r * kTcolProdWarps;
+                const int kg = it >> 1, half = it & 1;
+                const int n = 64 * half + 16 * c4;
+                fast[r] = false;
+                if (it >= ITEMS || n < n_lo || n >= n_hi) continue;
+                const int sy = border_index(y0 + 8 * kg + r8, a.H, a.border);
+                const int gx = x0 + n;
+                if (sy >= 0 && gx >= 0 && gx + 16 <= a.rowlen) {
+                    raw[r] = __ldg(reinterpret_cast<const uint4*>(a.src + (long long)sy * a.spitch + gx));
+                    fast[r] = true;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < PER; ++r) {
+                const int it = pw + r * kTcolProdWarps;
+                const int kg = it >> 1, half = it & 1;
+                const int n = 64 * half + 16 * c4;
+                if (it >= ITEMS || n < n_lo || n >= n_hi) continue;
+                unsigned h[8];
+                if (fast[r]) {
+                    tcol_cvt_word(raw[r].x, h[0], h[1]);
+                    tcol_cvt_word(raw[r].y, h[2], h[3]);
+                    tcol_cvt_word(raw[r].z, h[4], h[5]);
+                    tcol_cvt_word(raw[r].w, h[6], h[7]);
+                } else {
+                    const int sy = border_index(y0 + 8 * kg + r8, a.H, a.border);
+                    const unsigned char* srow = sy >= 0 ? a.src + (long long)sy * a.spitch : nullptr;
+                    const int gx = x0 + n;
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        h[e] = (unsigned)tcol_sample_h(a, srow, gx + 2 * e, C) |
+                               ((unsigned)tcol_sample_h(a, srow, gx + 2 * e + 1, C) << 16);
+                }
+                const int k = 8 * kg + r8;
+                *reinterpret_cast<uint4*>(B + tcol_b_off(n, k)) = make_uint4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint4*>(B + tcol_b_off(n + 8, k)) = make_uint4(h[4], h[5], h[6], h[7]);
+            }
+            fence_async_smem();
+            mbar_arrive(&bfull[bb]);
+            ++g;
+        }
+    } else {
+        // ------------------------------------------------------------ row pass
+        const int rw = warp - 1 - kTcolProdWarps;  // 0..7
+        const int q = warp & 3;                    // tensor-memory lane quarter of this warp
+        const int h = rw >> 2;                     // which half of the slab's columns
+        const uint32_t tlane = tbase + ((uint32_t)(32 * q) << 16);
+        TcolWalk walk(u0, u1, a.ns);
+        TcolStep st, prev{0, 0, 0};
+        int g = 0, ga = 0;  // step index, and the index of the current run's left halo
+        auto release = [&](int gg) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[gg & 3]);
+        };
+        while (walk.next(st)) {
+            // warp-uniform decisions: every lane leaves together, so no
+            // .sync.aligned instruction below runs with part of the warp
+            if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
+            const bool ok = tcol_wait(&tfull[g & 3], (unsigned)(g >> 2) & 1u, a, abort_flag);
+            if (!__all_sync(0xffffffffu, ok)) break;
+            tc_fence_after();
+            if (st.kind == 0) ga = g;
+            if (prev.kind == 1 && st.kind != 0) {
+                // row pass of slab prev (step g-1): buffers g-2, g-1, g
+                const int m = 32 * q + lane;
+                const int y = prev.band * kTcolM + m;
+                const int xs = prev.slab * kTcolN + 64 * h;  // first output sample of this thread
+                // column group rg (relative to 64h, in 16s) -> tensor-memory address
+                auto gaddr = [&](int rg) -> uint32_t {
+                    const int col = 64 * h + 16 * rg;  // relative to slab g-1's buffer, may leave [0,128)
+                    const int dg = col < 0 ? -1 : (col >= kTcolN ? 1 : 0);
+                    const int buf = (g - 1 + dg) & 3;
+                    return tlane + (uint32_t)(buf * kTcolN + (col - dg * kTcolN));
+                };
+                float v[NG][16];
+                __syncwarp();
+                static_for<0, 2 * GH + 1>([&](auto I) {
+                    constexpr int i = decltype(I)::value;
+                    tcol_ld16(gaddr(i - GH), v[i]);
+                });
+                static_for<0, 2 * GH + 1>([&](auto I) { tcol_ld_wait(v[decltype(I)::value]); });
+                unsigned char* drow = a.dst + (long long)y * a.dpitch;
+                const bool row_ok = y < a.H;
+                static_for<0, 4>([&](auto J) {
+                    constexpr int j = decltype(J)::value;
+                    // prefetch the group chunk j+1 needs last
+                    __syncwarp();
+                    if constexpr (j + GH + 1 < 4 + GH) tcol_ld16(gaddr(j + GH + 1), v[j + 2 * GH + 1]);
+                    unsigned words[4];
+#pragma unroll
+                    for (int t4 = 0; t4 < 4; ++t4) {
+                        unsigned wd = 0;
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) {
+                            const int o = 16 * j + 4 * t4 + t;  // output, relative to 64h
+                            float acc = a.off;
+#pragma unroll
+                            for (int i = 0; i < K; ++i) {
+                                const int col = o + C * (i - K / 2) + 16 * GH;  // into v, group 0 = rg -GH
+                                acc = fmaf(a.kx[i], v[col >> 4][col & 15], acc);
+                            }
+                            if (a.clamp) acc = fminf(fmaxf(acc, 0.f), 255.f);
+                            const float r = __fadd_rd(acc, 8388608.0f);
+                            wd = __byte_perm(wd, __float_as_uint(r), byte_insert_sel(t));
+                        }
+                        words[t4] = wd;
+                    }
+                    const int xo = xs + 16 * j;
+                    if (row_ok && xo < a.rowlen) {
+                        if (a.vec_store && xo + 16 <= a.rowlen) {
+                            *reinterpret_cast<uint4*>(drow + xo) = make_uint4(words[0], words[1], words[2], words[3]);
+                        } else {
+                            for (int e = 0; e < 16 && xo + e < a.rowlen; ++e)
+                                drow[xo + e] = (unsigned char)(words[e >> 2] >> (8 * (e & 3)));
+                        }
+                    }
+                    __syncwarp();
+                    if constexpr (j + GH + 1 < 4 + GH) tcol_ld_wait(v[j + 2 * GH + 1]);
+                });
+                (void)R;
+            }
+            // buffers no longer read: step g-2 when it belongs to this run, and
+            // at the run's end its last two
+            __syncwarp();
+            if (st.kind != 0 && g - 2 >= ga) release(g - 2);
+            if (st.kind == 2) {
+                release(g - 1);
+                release(g);
+            }
+            prev = st;
+            ++g;
+        }
+    }
+
+    // ---- teardown: every MMA complete before the tensor memory is freed
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        bool drained = true;
+        if (lane == 0) {
+            // every issued MMA completes in microseconds; the bound is 8 waits' worth
+            drained = mbar_try_wait(drain, 0);
+            const unsigned long long t0 = tcol_clock_ns();
+            while (!drained && tcol_clock_ns() - t0 <= 8 * a.wait_ns) drained = mbar_try_wait(drain, 0);
+            if (!drained && a.err) atomicCAS(a.err, 0u, kErrTcolDrain);
+        }
+        drained = __shfl_sync(0xffffffffu, drained ? 1 : 0, 0) != 0;
+        tc_fence_after();
+        if (drained) tmem_dealloc(tbase, kTcolTmemCols);
+    }
+}
+
+namespace {
+
+template <int K, int C>
+cudaError_t tcol_launch_kc(const TcolArgs& a, cudaStream_t s) {
+    static unsigned done = 0;
+    cudaError_t e = ensure_smem_attr((const void*)sep_tcol_kernel<K, C>, tcol_smem(K), &done);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const int grid = a.units < sms ? a.units : sms;
+    sep_tcol_kernel<K, C><<<grid, kTcolThreads, tcol_smem(K), s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int K>
+bool tcol_launch_k(int C, const TcolArgs& a, cudaStream_t s, cudaError_t* e) {
+    if (C == 1) *e = tcol_launch_kc<K, 1>(a, s);
+    else if (C == 3) *e = tcol_launch_kc<K, 3>(a, s);
+    else if (C == 4) *e = tcol_launch_kc<K, 4>(a, s);
+    else return false;
+    return true;
+}
+
+}  // namespace
+
+// (K, C) combinations instantiated: the row pass reaches at most 32 columns
+// either side (C * (K/2) <= 32).
+bool sep_tcol_supported(int K, int C) {
+    if (!(C == 1 || C == 3 || C == 4)) return false;
+    if (!(K == 5 || K == 13)) return false;
+    return C * (K / 2) <= 32;
+}
+
+// Launches the tensor-core column-pass kernel for uint8 -> uint8 with K
+// centred taps per axis on C channels; false when the call is outside what
+// it covers (the caller then uses the CUDA-core kernel).
+bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpitch, int W, int H, int C,
+                     const double* kx, const double* ky, int K, int border, double delta, double bv, int clamp,
+                     cudaStream_t s, cudaError_t* err) {
+    if (!sep_tcol_supported(K, C)) return false;
+    if (((uintptr_t)src & 15) || (spitch & 15) || spitch <= 0 || spitch >= (1LL << 40)) return false;
+    if (dpitch <= 0 || dpitch >= (1LL << 40)) return false;
+    if (border == IPFC_BORDER_CONSTANT && !(bv == std::floor(bv) && std::fabs(bv - 128.0) <= 2048.0)) return false;
+    double mx = 0, sy = 0, sx = 0;
+    for (int j = 0; j < K; ++j) {
+        if (!std::isfinite(ky[j]) || !std::isfinite(kx[j])) return false;
+        mx = std::fmax(mx, std::fabs(ky[j]));
+        sy += ky[j];
+        sx += kx[j];
+    }
+    int ex = 0;
+    if (mx > 0) {
+        int e2 = 0;
+        std::frexp(mx, &e2);  // mx = f 2^e2, f in [0.5, 1)
+        ex = 14 - e2;         // largest scaled tap in [2^13, 2^14)
+    }
+    TcolArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.src = static_cast<const unsigned char*>(src);
+    a.spitch = spitch;
+    a.dst = static_cast<unsigned char*>(dst);
+    a.dpitch = dpitch;
+    a.W = W;
+    a.H = H;
+    a.rowlen = W * C;
+    a.border = border;
+    a.bvh = __half_as_ushort(__double2half(border == IPFC_BORDER_CONSTANT ? bv - 128.0 : 0.0));
+    a.nb = (H + kTcolM - 1) / kTcolM;
+    a.ns = (a.rowlen + kTcolN - 1) / kTcolN;
+    a.units = a.nb * a.ns;
+    a.clamp = clamp;
+    a.vec_store = (((uintptr_t)dst & 15) == 0 && (dpitch & 15) == 0) ? 1 : 0;
+    a.off = (float)(128.0 * sy * sx + delta + 0.5);
+    a.wait_ns = 250ull * 1000 * 1000;  // 250 ms: far above any legitimate stage wait
+    for (int j = 0; j < K; ++j) {
+        const double w = std::ldexp(ky[j], ex);
+        const __half hi = __double2half(w);
+        const __half lo = __double2half(w - (double)__half2float(hi));
+        a.ahi[j] = __half_as_ushort(hi);
+        a.alo[j] = __half_as_ushort(lo);
+        a.kx[j] = std::ldexp((float)kx[j], -ex);
+    }
+    a.err = device_error_word();
+    cudaError_t e = cudaErrorInvalidValue;
+    bool launched = false;
+    switch (K) {
+        case 5: launched = tcol_launch_k<5>(C, a, s, &e); break;
+        case 13: launched = tcol_launch_k<13>(C, a, s, &e); break;
+        default: return false;
+    }
+    if (!launched) return false;
+    *err = e;
+    return true;
+}
+
+}  // namespace ipfc

@@ -4,7 +4,11 @@ test_gpu_parity.test_generic_separable_path with IPFC_SEP_PATH=generic (the
 generic fused / two-pass kernels) and by test_tc_separable_path with
 IPFC_SEP_PATH=tc (the tensor-core column-pass kernel), so those kernels are
 checked as well as the default one.  With --fullsize it also checks
-gaussianBlur sigma=2 on 1920x1080x3 and 3840x2160x3 uint8 within 1 LSB."""
+gaussianBlur sigma=2 on 1920x1080x3 and 3840x2160x3 uint8 within 1 LSB.
+With --sweep it also runs uint8 sepFilter2D over awkward shapes (1x1,
+widths and heights that are no multiple of the kernels' tiles), 1, 3 and 4
+channels, 5 and 13 taps (non-negative and signed), every border (Constant
+with an integer border value) against the oracle within 1 LSB."""
 import os
 import sys
 
@@ -41,5 +45,39 @@ def main():
             print(f"gaussian {w}x{h}x3 ok: mismatch rate {rate:.3e}")
 
 
+def sweep():
+    import numpy as np
+
+    import oracle
+
+    orc = oracle.restatement()
+    rng = np.random.default_rng(2027)
+    shapes = [(1, 1), (7, 3), (129, 130), (300, 257), (1000, 131), (43, 600)]
+    n = 0
+    for c in (1, 3, 4):
+        for w, h in shapes:
+            img = oracle.random_image(w, h, c, np.uint8, 31 * w + h + c)
+            for k in (5, 13):
+                for signed in (False, True):
+                    kx = rng.random(k) + (-0.3 if signed else 0.0)
+                    ky = rng.random(k) + (-0.3 if signed else 0.0)
+                    if signed:  # keep the sums well away from 0 before normalising
+                        kx[k // 2] += 2.0
+                        ky[k // 2] += 2.0
+                    kx /= kx.sum()
+                    ky /= ky.sum()
+                    for b in oracle.BORDERS:
+                        bv = 37.0 if b == oracle.CONSTANT else 0.0
+                        want = orc.sep_filter(img, kx, ky, border=b, delta=0.25, border_value=bv)
+                        got = ipf.sepFilter2D(img, kx, ky, ipf.BorderMode(b), 0.25, bv)
+                        d = np.abs(got.astype(np.int32) - want.astype(np.int32))
+                        if d.max(initial=0) > 1:
+                            raise SystemExit(f"sweep {w}x{h}x{c} k{k} signed={signed} border {b}: max {d.max()}")
+                        n += 1
+    print(f"{n} sweep cases ok")
+
+
 if __name__ == "__main__":
     main()
+    if "--sweep" in sys.argv:
+        sweep()

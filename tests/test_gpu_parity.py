@@ -255,6 +255,25 @@ def test_generic_separable_path(gpu):
     assert "separable cases ok (generic path)" in r.stdout
 
 
+def test_tcol_separable_path(gpu):
+    """The kernel with the column pass on tcgen05 and the row pass out of
+    tensor memory (sep_tcol.cu), forced for every uint8 separable call it
+    covers: every separable golden case, the full-size uint8 Gaussians and a
+    sweep of awkward shapes, channels, tap signs and borders."""
+    import os
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    env = dict(os.environ, IPFC_SEP_PATH="tcol")
+    r = subprocess.run([sys.executable, os.path.join(here, "sep_generic_check.py"), "--fullsize", "--sweep"],
+                       env=env, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    assert "separable cases ok (tcol path)" in r.stdout and "3840x2160x3 ok" in r.stdout
+    assert "sweep cases ok" in r.stdout
+    print(r.stdout)
+
+
 def test_tc_separable_path(gpu):
     """The tensor-core column-pass kernel (opt-in) against every separable
     golden case and the full-size uint8 Gaussians."""

@@ -8,6 +8,9 @@ the oracle's C restatement:
   to 256 and on sampled lengths up to the C ABI's limit of 2^30 - 1 samples
   per row, for all five border modes, and its interleaved form
   (border_sample) for 1 to 4 channels;
+* tcol_layout_check.cu: the shared-memory operands and descriptors of the
+  tensor-core separable kernel (csrc/sep_tcol.cuh), every MMA emulated from
+  the descriptor bits under the canonical layouts, and its step walk;
 * saturate_check.cu: the store rounding (sat_from_f) against saturate_cast
   (include/ipf/core.hpp:69-103) on all 2^32 float bit patterns, to uint8,
   uint16 and int16.
@@ -60,3 +63,7 @@ def test_border_index_matches_oracle(tmp_path):
 
 def test_saturate_matches_oracle_on_every_float(tmp_path):
     assert run_check(tmp_path, "saturate_check") == f"ok {3 * (1 << 32)}"
+
+
+def test_tcol_operand_layout(tmp_path):
+    assert run_check(tmp_path, "tcol_layout_check").startswith("ok ")
