@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/ipfc.h"
+#include "api_internal.h"
 #include "filter2d_tc.cuh"
 #include "kernels.cuh"
 #include "sep_fast_launch.cuh"
@@ -62,13 +63,13 @@ size_t elem_bytes(int dt) {
     }
 }
 
-static bool dtype_supported(int dt) { return dt == IPFC_U8 || dt == IPFC_U16 || dt == IPFC_I16 || dt == IPFC_F32; }
+static bool dtype_supported(int dt) { return dt >= IPFC_U8 && dt <= IPFC_F64; }
 
-static long long row_bytes(const ipfc_image* im) {
+long long row_bytes(const ipfc_image* im) {
     return (long long)im->width * im->channels * (long long)elem_bytes(im->dtype);
 }
 
-static long long pitch_of(const ipfc_image* im) { return im->pitch > 0 ? im->pitch : row_bytes(im); }
+long long pitch_of(const ipfc_image* im) { return im->pitch > 0 ? im->pitch : row_bytes(im); }
 
 // ---------------------------------------------------------------------------
 // Device memory: stream-ordered allocations from the device's default pool,
@@ -130,7 +131,7 @@ unsigned* device_error_word() {
 }
 
 // Reads and clears the error word after the stream has drained.
-static int take_device_error(cudaStream_t s, const char* fn) {
+int take_device_error(cudaStream_t s, const char* fn) {
     unsigned* w = device_error_word();
     if (!w) return IPFC_OK;
     unsigned v = 0;
@@ -145,16 +146,9 @@ static int take_device_error(cudaStream_t s, const char* fn) {
                      v);
 }
 
-// A device view of an image: the caller's memory, or a staged copy.
-struct DevView {
-    void* ptr = nullptr;
-    long long pitch = 0;
-    bool owned = false;
-};
+long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
-static long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
-
-static int view_in(const ipfc_image* im, cudaStream_t s, DevView* v, const char* fn) {
+int view_in(const ipfc_image* im, cudaStream_t s, DevView* v, const char* fn) {
     if (im->mem == IPFC_MEM_DEVICE) {
         v->ptr = im->data;
         v->pitch = pitch_of(im);
@@ -170,7 +164,7 @@ static int view_in(const ipfc_image* im, cudaStream_t s, DevView* v, const char*
     return IPFC_OK;
 }
 
-static int view_out(const ipfc_image* im, cudaStream_t s, DevView* v, const char* fn) {
+int view_out(const ipfc_image* im, cudaStream_t s, DevView* v, const char* fn) {
     if (im->mem == IPFC_MEM_DEVICE) {
         v->ptr = im->data;
         v->pitch = pitch_of(im);
@@ -185,7 +179,7 @@ static int view_out(const ipfc_image* im, cudaStream_t s, DevView* v, const char
 
 // Copies a staged result back to host memory, releases staging memory and,
 // when any side lives in host memory, waits for the stream.
-static int finish(const ipfc_image* dst, DevView* in, DevView* out, cudaStream_t s, const char* fn) {
+int finish(const ipfc_image* dst, DevView* in, DevView* out, cudaStream_t s, const char* fn) {
     cudaError_t e = cudaSuccess;
     if (out->owned) {
         e = cudaMemcpy2DAsync(dst->data, (size_t)pitch_of(dst), out->ptr, (size_t)out->pitch, (size_t)row_bytes(dst),
@@ -211,8 +205,7 @@ int check_pair(const ipfc_image* src, const ipfc_image* dst, const char* fn, boo
     if (dst->width != src->width || dst->height != src->height || dst->channels != src->channels)
         return set_error(IPFC_ERR_INVALID, "ipf: %s: destination shape does not match source", fn);
     if (!dtype_supported(src->dtype) || !dtype_supported(dst->dtype))
-        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: element type not provided by this build (u8, u16, i16, f32)",
-                         fn);
+        return set_error(IPFC_ERR_UNSUPPORTED, "ipf: %s: unknown element type code", fn);
     if (same_type && src->dtype != dst->dtype)
         return set_error(IPFC_ERR_INVALID, "ipf: %s: source and destination types differ", fn);
     if ((src->mem != IPFC_MEM_HOST && src->mem != IPFC_MEM_DEVICE) ||
@@ -293,6 +286,9 @@ cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spit
 bool sep_tc_launch(const void* src, long long spitch, void* dst, long long dpitch, int W, int H, int C,
                    const double* kx, const double* ky, int K, int border, double delta, double bv, int clamp,
                    cudaStream_t s, cudaError_t* err);
+bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpitch, int W, int H, int C,
+                     const double* kx, const double* ky, int K, int border, double delta, double bv, int clamp,
+                     cudaStream_t s, cudaError_t* err);
 
 // Kernel selection for separable filters.  Default: the CUDA-core fast
 // kernel where it is instantiated, else the generic kernels.
@@ -302,7 +298,10 @@ bool sep_tc_launch(const void* src, long long spitch, void* dst, long long dpitc
 static int sep_path_mode() {
     static const int mode = [] {  // read once, thread-safe initialisation
         const char* v = std::getenv("IPFC_SEP_PATH");
-        return (v && std::strcmp(v, "generic") == 0) ? 1 : (v && std::strcmp(v, "tc") == 0) ? 3 : 0;
+        return (v && std::strcmp(v, "generic") == 0) ? 1
+               : (v && std::strcmp(v, "tc") == 0)    ? 3
+               : (v && std::strcmp(v, "tcol") == 0)  ? 4
+                                                     : 0;
     }();
     return mode;
 }
@@ -398,10 +397,14 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
         sep_tc_launch(in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, kx, ky, kw, border,
                       delta, bv, f.clamp, s, e))
         return true;
+    if (sep_path_mode() == 4 && src->dtype == IPFC_U8 && dst->dtype == IPFC_U8 &&
+        sep_tcol_launch(in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, kx, ky, kw,
+                        border, delta, bv, f.clamp, s, e))
+        return true;
     return sep_fast_dispatch(kw, src->channels, src->dtype, dst->dtype, f, s, e);
 }
-static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh, int ax,
-                   int ay, int border, double delta, double bv, cudaStream_t s, const char* fn) {
+int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh, int ax, int ay,
+            int border, double delta, double bv, cudaStream_t s, const char* fn, bool force_fp64) {
     if (!kx || !ky || kw <= 0 || kh <= 0)
         return set_error(IPFC_ERR_INVALID, "ipf: separable filter: empty kernel");
     if (border < IPFC_BORDER_CONSTANT || border > IPFC_BORDER_WRAP)
@@ -424,8 +427,20 @@ static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int
     a.border = border;
     a.delta = (float)delta;
     a.bv = (float)bv;
-    for (int i = 0; i < kw && i < kSepMaxParamTaps; ++i) a.kx[i] = (float)kx[i];
-    for (int j = 0; j < kh && j < kSepMaxParamTaps; ++j) a.ky[j] = (float)ky[j];
+    a.deltad = delta;
+    a.bvd = bv;
+    for (int i = 0; i < kw && i < kSepMaxParamTaps; ++i) {
+        a.kx[i] = (float)kx[i];
+        a.kxd[i] = kx[i];
+    }
+    for (int j = 0; j < kh && j < kSepMaxParamTaps; ++j) {
+        a.ky[j] = (float)ky[j];
+        a.kyd[j] = ky[j];
+    }
+    // FP64 accumulation (the reference's own arithmetic, bit-identical
+    // results) for int32 / double images, and when a composite op asks for
+    // it to reproduce the reference's intermediate exactly
+    const bool wide = force_fp64 || sep_wide(src->dtype, dst->dtype);
     DevView in, out;
     if ((rc = view_in(src, s, &in, fn))) return rc;
     if ((rc = view_out(dst, s, &out, fn))) {
@@ -436,25 +451,32 @@ static int run_sep(const ipfc_image* src, ipfc_image* dst, const double* kx, int
     a.spitch = in.pitch;
     a.dst = out.ptr;
     a.dpitch = out.pitch;
-    float* dtaps = nullptr;
-    float* scratch = nullptr;
+    unsigned char* dtaps = nullptr;  // kw + kh taps, float or (FP64 calls) double
+    void* scratch = nullptr;
     cudaError_t e = cudaSuccess;
-    if (run_sep_fast(src, dst, in, out, kx, kw, ky, kh, ax, ay, border, delta, bv, s, &e)) {
+    if (!wide && run_sep_fast(src, dst, in, out, kx, kw, ky, kh, ax, ay, border, delta, bv, s, &e)) {
         rc = finish(dst, &in, &out, s, fn);
         if (e != cudaSuccess) return cuda_status(e, fn);
         return rc;
     }
-    if (sep_needs_scratch(a)) {
-        std::vector<float> taps((size_t)kw + kh);
-        for (int i = 0; i < kw; ++i) taps[i] = (float)kx[i];
-        for (int j = 0; j < kh; ++j) taps[kw + j] = (float)ky[j];
-        e = cudaMallocAsync((void**)&dtaps, taps.size() * sizeof(float), s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(dtaps, taps.data(), taps.size() * sizeof(float),
-                                                  cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess)
-            e = cudaMallocAsync((void**)&scratch, sizeof(float) * (size_t)a.W * a.C * a.H, s);
+    const size_t tsz = wide ? sizeof(double) : sizeof(float);
+    if (sep_needs_scratch(a, wide)) {
+        std::vector<unsigned char> taps(((size_t)kw + kh) * tsz);
+        for (int i = 0; i < kw + kh; ++i) {
+            const double v = i < kw ? kx[i] : ky[i - kw];
+            if (wide) std::memcpy(&taps[(size_t)i * tsz], &v, tsz);
+            else {
+                const float f = (float)v;
+                std::memcpy(&taps[(size_t)i * tsz], &f, tsz);
+            }
+        }
+        e = cudaMallocAsync((void**)&dtaps, taps.size(), s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dtaps, taps.data(), taps.size(), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMallocAsync(&scratch, tsz * (size_t)a.W * a.C * a.H, s);
     }
-    if (e == cudaSuccess) e = sep_launch(src->dtype, dst->dtype, a, dtaps, dtaps ? dtaps + kw : nullptr, scratch, s);
+    if (e == cudaSuccess)
+        e = sep_launch(src->dtype, dst->dtype, a, dtaps, dtaps ? dtaps + (size_t)kw * tsz : nullptr, scratch, s,
+                       force_fp64);
     if (dtaps) cudaFreeAsync(dtaps, s);
     if (scratch) cudaFreeAsync(scratch, s);
     rc = finish(dst, &in, &out, s, fn);
@@ -530,7 +552,7 @@ int ipfc_structuring_element(int shape, int width, int height, uint8_t* out) {
 int ipfc_sep_filter2d(const ipfc_image* src, ipfc_image* dst, const double* kx, int kw, const double* ky, int kh,
                       int ax, int ay, int border, double delta, double border_value, void* stream) {
     return run_sep(src, dst, kx, kw, ky, kh, ax, ay, border, delta, border_value, (cudaStream_t)stream,
-                   "sepFilter2D");
+                   "sepFilter2D", false);
 }
 
 int ipfc_gaussian_blur(const ipfc_image* src, ipfc_image* dst, double sigma_x, double sigma_y, int ksize, int border,
@@ -540,7 +562,7 @@ int ipfc_gaussian_blur(const ipfc_image* src, ipfc_image* dst, double sigma_x, d
     if (gaussian_taps(sigma_x, ksize, kx)) return IPFC_ERR_INVALID;
     if (gaussian_taps(sigma_y, ksize, ky)) return IPFC_ERR_INVALID;
     return run_sep(src, dst, kx.data(), (int)kx.size(), ky.data(), (int)ky.size(), -1, -1, border, 0.0, 0.0,
-                   (cudaStream_t)stream, "gaussianBlur");
+                   (cudaStream_t)stream, "gaussianBlur", false);
 }
 
 int ipfc_sobel(const ipfc_image* src, ipfc_image* dst, int dx, int dy, int ksize, double scale, int border,
@@ -555,11 +577,15 @@ int ipfc_sobel(const ipfc_image* src, ipfc_image* dst, int dx, int dy, int ksize
     }
     for (double& v : kx) v *= scale;
     return run_sep(src, dst, kx.data(), (int)kx.size(), ky.data(), (int)ky.size(), -1, -1, border, 0.0, 0.0,
-                   (cudaStream_t)stream, "sobel");
+                   (cudaStream_t)stream, "sobel", false);
 }
 
-int ipfc_box_filter(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int normalize, int border,
-                    double border_value, void* stream) {
+}  // extern "C"
+
+namespace ipfc {
+
+int run_box(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int normalize, int border, double border_value,
+            cudaStream_t s, bool force_fp64) {
     const char* fn = "boxFilter";
     if (kw <= 0 || kh <= 0) return set_error(IPFC_ERR_INVALID, "ipf: boxFilter: kernel size must be positive");
     if (border < IPFC_BORDER_CONSTANT || border > IPFC_BORDER_WRAP)
@@ -567,7 +593,6 @@ int ipfc_box_filter(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int 
     int rc = check_pair(src, dst, fn, false);
     if (rc == -1) return IPFC_OK;
     if (rc) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
     BoxArgs a;
     std::memset(&a, 0, sizeof(a));
     a.W = src->width;
@@ -580,11 +605,13 @@ int ipfc_box_filter(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int 
     a.border = border;
     a.normalize = normalize ? 1 : 0;
     a.bv = (float)border_value;
+    a.bvd = border_value;
     const double n = (double)kw * kh;
     const double scale = normalize ? 1.0 / n : 1.0;
     a.scale_hi = (float)scale;
     a.scale_lo = (float)(scale - (double)a.scale_hi);
-    const bool int_src = src->dtype != IPFC_F32;
+    a.scaled = scale;
+    const bool int_src = src->dtype == IPFC_U8 || src->dtype == IPFC_U16 || src->dtype == IPFC_I16;
     const double maxval = src->dtype == IPFC_U8 ? 255.0 : (src->dtype == IPFC_U16 ? 65535.0 : 32768.0);
     const bool bv_int = std::floor(border_value) == border_value && std::fabs(border_value) <= 65535.0;
     const bool exact = int_src && bv_int && n * std::fmax(maxval, std::fabs(border_value)) < 2147483647.0;
@@ -609,10 +636,19 @@ int ipfc_box_filter(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int 
     a.spitch = in.pitch;
     a.dst = out.ptr;
     a.dpitch = out.pitch;
-    cudaError_t e = box_launch(src->dtype, dst->dtype, a, exact, s);
+    cudaError_t e = box_launch(src->dtype, dst->dtype, a, exact && !force_fp64, s, force_fp64);
     rc = finish(dst, &in, &out, s, fn);
     if (e != cudaSuccess) return cuda_status(e, fn);
     return rc;
+}
+
+}  // namespace ipfc
+
+extern "C" {
+
+int ipfc_box_filter(const ipfc_image* src, ipfc_image* dst, int kw, int kh, int normalize, int border,
+                    double border_value, void* stream) {
+    return run_box(src, dst, kw, kh, normalize, border, border_value, (cudaStream_t)stream, false);
 }
 
 }  // extern "C"
@@ -676,6 +712,8 @@ static int run_filter2d(const ipfc_image* src, ipfc_image* dst, const float* ker
     a.border = border;
     a.delta = (float)delta;
     a.bv = (float)border_value;
+    a.deltad = delta;
+    a.bvd = border_value;
     a.ntaps = (int)taps.size();
     a.dense = a.ntaps == kw * kh;
     DevView in, out;

@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/ipfc.h"
 
 namespace ipfc {
@@ -90,10 +92,30 @@ template <> struct Elem<int16_t> {
     static constexpr float lo = -32768.f, hi = 32767.f;
     static constexpr bool is_int = true;
 };
+template <> struct Elem<int32_t> {
+    static constexpr int code = IPFC_I32;
+    static constexpr float lo = -2147483648.f, hi = 2147483647.f;  // float form: not used for rounding
+    static constexpr double dlo = -2147483648.0, dhi = 2147483647.0;
+    static constexpr bool is_int = true;
+};
 template <> struct Elem<float> {
     static constexpr int code = IPFC_F32;
     static constexpr float lo = -3.402823466e38f, hi = 3.402823466e38f;
     static constexpr bool is_int = false;
+};
+template <> struct Elem<double> {
+    static constexpr int code = IPFC_F64;
+    static constexpr bool is_int = false;
+};
+
+// Accumulator of the generic kernels: FP64 when either side is a 32-bit
+// integer or double image (the reference accumulates in FP64 throughout; FP32
+// cannot hold int32 samples exactly), FP32 otherwise.
+template <typename Tin, typename Tout>
+struct AccOf {
+    static constexpr bool wide = std::is_same<Tin, int32_t>::value || std::is_same<Tin, double>::value ||
+                                 std::is_same<Tout, int32_t>::value || std::is_same<Tout, double>::value;
+    using type = typename std::conditional<wide, double, float>::type;
 };
 
 template <typename T>
@@ -119,6 +141,33 @@ __host__ __device__ __forceinline__ T sat_from_f(float v) {
         return static_cast<T>(static_cast<int>(r));
     } else {
         return static_cast<T>(v);
+    }
+}
+
+// saturate_cast<T>(double) exactly as the reference evaluates it
+// (include/ipf/core.hpp:69-103): NaN -> 0; integers add -0.5 or +0.5 in FP64
+// (one rounding, as in the reference), saturate at the type's limits, then
+// truncate toward zero; float narrows with round-to-nearest; double is kept.
+template <typename T>
+__host__ __device__ __forceinline__ T sat_from_d(double v) {
+    if constexpr (std::is_same<T, double>::value) {
+        return v;
+    } else if constexpr (std::is_same<T, float>::value) {
+        return static_cast<float>(v);
+    } else {
+        if (!(v == v)) return T(0);
+        double lo, hi;
+        if constexpr (std::is_same<T, int32_t>::value) {
+            lo = Elem<T>::dlo;
+            hi = Elem<T>::dhi;
+        } else {
+            lo = (double)Elem<T>::lo;
+            hi = (double)Elem<T>::hi;
+        }
+        const double d = v < 0 ? v - 0.5 : v + 0.5;
+        if (d <= lo) return static_cast<T>(lo);
+        if (d >= hi) return static_cast<T>(hi);
+        return static_cast<T>(d);
     }
 }
 

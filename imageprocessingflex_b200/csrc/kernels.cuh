@@ -53,6 +53,7 @@ struct F2DArgs {
     int kw, kh, ax, ay;
     int border;
     float delta, bv;
+    double deltad, bvd;  // the same in FP64 (int32 / double images accumulate in FP64)
     int ntaps;       // non-zero taps
     int dense;       // 1 when every tap is non-zero (taps = kw*kh, row-major)
     const float4* taps;  // device: {w, dx, dy, 0} per non-zero tap, row-major order

@@ -10,7 +10,7 @@ constexpr int kThreads = 256;
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) median_kernel(const MedianArgs a, int TX, int TY) {
-    extern __shared__ float tile[];
+    extern __shared__ __align__(16) float tile[];
     median_tile<T>(a, TX, TY, blockIdx.x, blockIdx.y, tile);
 }
 
@@ -35,16 +35,17 @@ cudaError_t median_u8(const MedianArgs& a, cudaStream_t s) {
 
 template <typename T>
 cudaError_t median_typed(const MedianArgs& a, cudaStream_t s) {
+    constexpr size_t es = sizeof(typename median_detail::Store<T>::type);
     int TX = 128, TY = 32;
     size_t smem;
     for (;;) {
-        smem = median_tile_bytes(TX, TY, a.ksize, a.C);
+        smem = median_tile_bytes(TX, TY, a.ksize, a.C, es);
         if (smem <= 96 * 1024 || TY <= 1) break;
         TY /= 2;
     }
     while (smem > 96 * 1024 && TX > 32) {
         TX /= 2;
-        smem = median_tile_bytes(TX, TY, a.ksize, a.C);
+        smem = median_tile_bytes(TX, TY, a.ksize, a.C, es);
     }
     if (smem > 96 * 1024) return cudaErrorInvalidConfiguration;
     static unsigned done = 0;
@@ -65,7 +66,9 @@ cudaError_t median_launch(int dt, const MedianArgs& a, cudaStream_t s) {
         case IPFC_U8: return median_typed<uint8_t>(a, s);
         case IPFC_U16: return median_typed<uint16_t>(a, s);
         case IPFC_I16: return median_typed<int16_t>(a, s);
+        case IPFC_I32: return median_typed<int32_t>(a, s);
         case IPFC_F32: return median_typed<float>(a, s);
+        case IPFC_F64: return median_typed<double>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

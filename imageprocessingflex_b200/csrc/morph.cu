@@ -7,10 +7,11 @@ namespace ipfc {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kMorphU8VhgwFrom = 11;  // uint8 rect members per axis from which the generic tile takes over
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) morph_kernel(const MorphArgs a, int TX, int TY) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     if (a.is_rect) morph_rect_tile<T>(a, TX, TY, blockIdx.x, blockIdx.y, smem);
     else morph_list_tile<T>(a, TX, TY, blockIdx.x, blockIdx.y, smem);
 }
@@ -36,12 +37,17 @@ cudaError_t morph_u8_rect(const MorphCore& a, cudaStream_t s) {
 
 template <typename T>
 cudaError_t morph_typed(const MorphArgs& a, cudaStream_t s) {
+    constexpr size_t es = sizeof(typename MorphStore<T>::type);
     int TX = 128, TY = 32;
     size_t smem;
     for (;;) {
-        smem = morph_tile_bytes(TX, TY, a.sw, a.sh, a.C, a.is_rect != 0);
+        smem = morph_tile_bytes(TX, TY, a.sw, a.sh, a.C, a.is_rect != 0, es);
         if (smem <= 96 * 1024 || TY <= 1) break;
         TY /= 2;
+    }
+    while (smem > 96 * 1024 && TX > 32) {
+        TX /= 2;
+        smem = morph_tile_bytes(TX, TY, a.sw, a.sh, a.C, a.is_rect != 0, es);
     }
     if (smem > 96 * 1024) return cudaErrorInvalidConfiguration;
     static unsigned done = 0;
@@ -56,13 +62,18 @@ cudaError_t morph_typed(const MorphArgs& a, cudaStream_t s) {
 }  // namespace
 
 cudaError_t morph_launch(int dt, const MorphArgs& a, cudaStream_t s) {
-    if (dt == IPFC_U8 && a.is_rect && morph_u8_tile_bytes(256, 32, a.sw, a.sh, a.C) <= 96 * 1024)
+    // uint8 rectangles: the packed-byte tile's direct scans up to 9 members
+    // per axis; longer ones run van Herk / Gil-Werman in the generic tile
+    if (dt == IPFC_U8 && a.is_rect && a.sw < kMorphU8VhgwFrom && a.sh < kMorphU8VhgwFrom &&
+        morph_u8_tile_bytes(256, 32, a.sw, a.sh, a.C) <= 96 * 1024)
         return morph_u8_rect(a, s);
     switch (dt) {
         case IPFC_U8: return morph_typed<uint8_t>(a, s);
         case IPFC_U16: return morph_typed<uint16_t>(a, s);
         case IPFC_I16: return morph_typed<int16_t>(a, s);
+        case IPFC_I32: return morph_typed<int32_t>(a, s);
         case IPFC_F32: return morph_typed<float>(a, s);
+        case IPFC_F64: return morph_typed<double>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -29,35 +29,57 @@ struct FusedGeom {
     size_t smem;
 };
 
-FusedGeom fused_geom(const SepArgs& a) {
+FusedGeom fused_geom(const SepArgs& a, size_t esize) {
     FusedGeom g{128, 32, 0};
     for (;;) {
         const int RY = g.TY + a.kh - 1, SW = g.TX + (a.kw - 1) * a.C;
-        g.smem = sizeof(float) * ((size_t)RY * SW + (size_t)RY * g.TX);
+        g.smem = esize * ((size_t)RY * SW + (size_t)RY * g.TX);
         if (g.smem <= 96 * 1024 || g.TY <= 4) return g;
         g.TY /= 2;
     }
 }
 
-template <typename Tin, typename Tout>
+// One multiply-add of the accumulation.  FP32: fused.  FP64: a rounded
+// product then a rounded sum, the reference's own sequence (it is built
+// without FMA contraction), so FP64 results match it bit for bit.
+__device__ __forceinline__ float acc_madd(float acc, float k, float x) { return fmaf(k, x, acc); }
+__device__ __forceinline__ double acc_madd(double acc, double k, double x) {
+    return __dadd_rn(acc, __dmul_rn(k, x));
+}
+
+template <typename Tacc> __device__ __forceinline__ Tacc tap_x(const SepArgs& a, int i);
+template <> __device__ __forceinline__ float tap_x<float>(const SepArgs& a, int i) { return a.kx[i]; }
+template <> __device__ __forceinline__ double tap_x<double>(const SepArgs& a, int i) { return a.kxd[i]; }
+template <typename Tacc> __device__ __forceinline__ Tacc tap_y(const SepArgs& a, int j);
+template <> __device__ __forceinline__ float tap_y<float>(const SepArgs& a, int j) { return a.ky[j]; }
+template <> __device__ __forceinline__ double tap_y<double>(const SepArgs& a, int j) { return a.kyd[j]; }
+
+template <typename Tout>
+__device__ __forceinline__ Tout sat_acc(float v) { return sat_from_f<Tout>(v); }
+template <typename Tout>
+__device__ __forceinline__ Tout sat_acc(double v) { return sat_from_d<Tout>(v); }
+
+template <typename Tin, typename Tout, typename Tacc>
 __global__ void __launch_bounds__(kThreads) sep_fused_kernel(const SepArgs a, int TX, int TY) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) unsigned char smem_raw_sep[];
+    Tacc* smem = reinterpret_cast<Tacc*>(smem_raw_sep);
     const int RY = TY + a.kh - 1;
     const int SW = TX + (a.kw - 1) * a.C;
-    float* tin = smem;
-    float* th = smem + (size_t)RY * SW;
+    Tacc* tin = smem;
+    Tacc* th = smem + (size_t)RY * SW;
     const int rowlen = a.W * a.C;
     const int q0 = blockIdx.x * TX;
     const int y0 = blockIdx.y * TY;
-    load_tile<Tin, float>(tin, RY, SW, a.src, a.spitch, a.W, a.H, a.C, q0 - a.ax * a.C, y0 - a.ay, a.border, a.bv);
+    const Tacc bv = std::is_same<Tacc, double>::value ? (Tacc)a.bvd : (Tacc)a.bv;
+    load_tile<Tin, Tacc>(tin, RY, SW, a.src, a.spitch, a.W, a.H, a.C, q0 - a.ax * a.C, y0 - a.ay, a.border, bv);
     __syncthreads();
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int nt = blockDim.x * blockDim.y;
     for (int idx = tid; idx < RY * TX; idx += nt) {
         const int r = idx / TX, t = idx - r * TX;
-        const float* p = tin + (size_t)r * SW + t;
-        float acc = 0.f;
-        for (int i = 0; i < a.kw; ++i) acc = fmaf(a.kx[i], p[i * a.C], acc);
+        const Tacc* p = tin + (size_t)r * SW + t;
+        Tacc acc = 0;
+        for (int i = 0; i < a.kw; ++i) acc = acc_madd(acc, tap_x<Tacc>(a, i), p[i * a.C]);
         th[idx] = acc;
     }
     __syncthreads();
@@ -65,27 +87,28 @@ __global__ void __launch_bounds__(kThreads) sep_fused_kernel(const SepArgs a, in
         const int y = idx / TX, t = idx - y * TX;
         const int gy = y0 + y, gq = q0 + t;
         if (gy >= a.H || gq >= rowlen) continue;
-        const float* p = th + (size_t)y * TX + t;
-        float acc = a.delta;
-        for (int j = 0; j < a.kh; ++j) acc = fmaf(a.ky[j], p[(size_t)j * TX], acc);
-        row_ptr_mut<Tout>(a.dst, a.dpitch, gy)[gq] = sat_from_f<Tout>(acc);
+        const Tacc* p = th + (size_t)y * TX + t;
+        Tacc acc = std::is_same<Tacc, double>::value ? (Tacc)a.deltad : (Tacc)a.delta;
+        for (int j = 0; j < a.kh; ++j) acc = acc_madd(acc, tap_y<Tacc>(a, j), p[(size_t)j * TX]);
+        row_ptr_mut<Tout>(a.dst, a.dpitch, gy)[gq] = sat_acc<Tout>(acc);
     }
 }
 
 // Row pass of the two-pass form: h[y][q] for every in-image row y.
-template <typename Tin>
-__global__ void __launch_bounds__(kThreads) sep_rows_kernel(const SepArgs a, const float* __restrict__ kx,
-                                                            float* __restrict__ h) {
+template <typename Tin, typename Tacc>
+__global__ void __launch_bounds__(kThreads) sep_rows_kernel(const SepArgs a, const Tacc* __restrict__ kx,
+                                                            Tacc* __restrict__ h) {
     const int rowlen = a.W * a.C;
     const int y = blockIdx.y;
     const Tin* srow = row_ptr<Tin>(a.src, a.spitch, y);
+    const Tacc bv = std::is_same<Tacc, double>::value ? (Tacc)a.bvd : (Tacc)a.bv;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rowlen; q += gridDim.x * blockDim.x) {
-        float acc = 0.f;
+        Tacc acc = 0;
         const int base = q - a.ax * a.C;
         for (int i = 0; i < a.kw; ++i) {
             const int g = base + i * a.C;
             const int idx = ((unsigned)g < (unsigned)rowlen) ? g : border_sample(g, a.W, a.C, a.border);
-            acc = fmaf(kx[i], idx < 0 ? a.bv : to_f(srow[idx]), acc);
+            acc = acc_madd(acc, kx[i], idx < 0 ? bv : static_cast<Tacc>(srow[idx]));
         }
         h[(size_t)y * rowlen + q] = acc;
     }
@@ -93,70 +116,90 @@ __global__ void __launch_bounds__(kThreads) sep_rows_kernel(const SepArgs a, con
 
 // Column pass: a row outside the image reads borderValue * sum(kx) (the row
 // pass of a row that is borderValue everywhere), accumulated in tap order.
-template <typename Tout>
-__global__ void __launch_bounds__(kThreads) sep_cols_kernel(const SepArgs a, const float* __restrict__ kx,
-                                                            const float* __restrict__ ky,
-                                                            const float* __restrict__ h) {
+template <typename Tout, typename Tacc>
+__global__ void __launch_bounds__(kThreads) sep_cols_kernel(const SepArgs a, const Tacc* __restrict__ kx,
+                                                            const Tacc* __restrict__ ky,
+                                                            const Tacc* __restrict__ h) {
     const int rowlen = a.W * a.C;
     const int y = blockIdx.y;
-    float const_row = 0.f;
-    for (int i = 0; i < a.kw; ++i) const_row = fmaf(kx[i], a.bv, const_row);
+    const Tacc bv = std::is_same<Tacc, double>::value ? (Tacc)a.bvd : (Tacc)a.bv;
+    Tacc const_row = 0;
+    for (int i = 0; i < a.kw; ++i) const_row = acc_madd(const_row, kx[i], bv);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rowlen; q += gridDim.x * blockDim.x) {
-        float acc = a.delta;
+        Tacc acc = std::is_same<Tacc, double>::value ? (Tacc)a.deltad : (Tacc)a.delta;
         for (int j = 0; j < a.kh; ++j) {
             const int sy = border_index(y + j - a.ay, a.H, a.border);
-            acc = fmaf(ky[j], sy < 0 ? const_row : h[(size_t)sy * rowlen + q], acc);
+            acc = acc_madd(acc, ky[j], sy < 0 ? const_row : h[(size_t)sy * rowlen + q]);
         }
-        row_ptr_mut<Tout>(a.dst, a.dpitch, y)[q] = sat_from_f<Tout>(acc);
+        row_ptr_mut<Tout>(a.dst, a.dpitch, y)[q] = sat_acc<Tout>(acc);
     }
 }
 
-template <typename Tin, typename Tout>
-cudaError_t launch_typed(const SepArgs& a, const float* dkx, const float* dky, float* scratch, cudaStream_t s) {
+template <typename Tin, typename Tout, typename Tacc>
+cudaError_t launch_acc(const SepArgs& a, const void* dkx, const void* dky, void* scratch, cudaStream_t s) {
     const int rowlen = a.W * a.C;
-    if (!sep_needs_scratch(a)) {
-        const FusedGeom g = fused_geom(a);
+    if (!sep_needs_scratch(a, std::is_same<Tacc, double>::value)) {
+        const FusedGeom g = fused_geom(a, sizeof(Tacc));
         static unsigned done = 0;  // per instantiation, one bit per device
-        cudaError_t e = ensure_smem_attr((const void*)sep_fused_kernel<Tin, Tout>, 96 * 1024, &done);
+        cudaError_t e = ensure_smem_attr((const void*)sep_fused_kernel<Tin, Tout, Tacc>, 96 * 1024, &done);
         if (e != cudaSuccess) return e;
         dim3 grid((rowlen + g.TX - 1) / g.TX, (a.H + g.TY - 1) / g.TY);
         dim3 block(32, kThreads / 32);
-        sep_fused_kernel<Tin, Tout><<<grid, block, g.smem, s>>>(a, g.TX, g.TY);
+        sep_fused_kernel<Tin, Tout, Tacc><<<grid, block, g.smem, s>>>(a, g.TX, g.TY);
         return cudaGetLastError();
     }
+    if (!dkx || !dky || !scratch) return cudaErrorInvalidValue;
     const int bx = (rowlen + kThreads - 1) / kThreads;
     dim3 grid(bx < 64 ? bx : 64, a.H);
-    sep_rows_kernel<Tin><<<grid, kThreads, 0, s>>>(a, dkx, scratch);
-    sep_cols_kernel<Tout><<<grid, kThreads, 0, s>>>(a, dkx, dky, scratch);
+    sep_rows_kernel<Tin, Tacc><<<grid, kThreads, 0, s>>>(a, static_cast<const Tacc*>(dkx), static_cast<Tacc*>(scratch));
+    sep_cols_kernel<Tout, Tacc><<<grid, kThreads, 0, s>>>(a, static_cast<const Tacc*>(dkx),
+                                                          static_cast<const Tacc*>(dky),
+                                                          static_cast<const Tacc*>(scratch));
     return cudaGetLastError();
 }
 
+// Accumulator: FP64 for int32 / double images or when asked, FP32 otherwise.
+template <typename Tin, typename Tout>
+cudaError_t launch_typed(const SepArgs& a, const void* dkx, const void* dky, void* scratch, cudaStream_t s,
+                         bool fp64) {
+    if constexpr (AccOf<Tin, Tout>::wide) {
+        return launch_acc<Tin, Tout, double>(a, dkx, dky, scratch, s);
+    } else {
+        if (fp64) return launch_acc<Tin, Tout, double>(a, dkx, dky, scratch, s);
+        return launch_acc<Tin, Tout, float>(a, dkx, dky, scratch, s);
+    }
+}
+
 template <typename Tin>
-cudaError_t launch_out(int ddt, const SepArgs& a, const float* dkx, const float* dky, float* scratch,
-                       cudaStream_t s) {
+cudaError_t launch_out(int ddt, const SepArgs& a, const void* dkx, const void* dky, void* scratch, cudaStream_t s,
+                       bool fp64) {
     switch (ddt) {
-        case IPFC_U8: return launch_typed<Tin, uint8_t>(a, dkx, dky, scratch, s);
-        case IPFC_U16: return launch_typed<Tin, uint16_t>(a, dkx, dky, scratch, s);
-        case IPFC_I16: return launch_typed<Tin, int16_t>(a, dkx, dky, scratch, s);
-        case IPFC_F32: return launch_typed<Tin, float>(a, dkx, dky, scratch, s);
+        case IPFC_U8: return launch_typed<Tin, uint8_t>(a, dkx, dky, scratch, s, fp64);
+        case IPFC_U16: return launch_typed<Tin, uint16_t>(a, dkx, dky, scratch, s, fp64);
+        case IPFC_I16: return launch_typed<Tin, int16_t>(a, dkx, dky, scratch, s, fp64);
+        case IPFC_I32: return launch_typed<Tin, int32_t>(a, dkx, dky, scratch, s, fp64);
+        case IPFC_F32: return launch_typed<Tin, float>(a, dkx, dky, scratch, s, fp64);
+        case IPFC_F64: return launch_typed<Tin, double>(a, dkx, dky, scratch, s, fp64);
         default: return cudaErrorInvalidValue;
     }
 }
 
 }  // namespace
 
-bool sep_needs_scratch(const SepArgs& a) {
+bool sep_needs_scratch(const SepArgs& a, bool wide) {
     if (a.kw > kSepMaxParamTaps || a.kh > kSepMaxParamTaps) return true;
-    return fused_geom(a).smem > 96 * 1024;
+    return fused_geom(a, wide ? sizeof(double) : sizeof(float)).smem > 96 * 1024;
 }
 
-cudaError_t sep_launch(int sdt, int ddt, const SepArgs& a, const float* dkx, const float* dky, float* scratch,
-                       cudaStream_t s) {
+cudaError_t sep_launch(int sdt, int ddt, const SepArgs& a, const void* dkx, const void* dky, void* scratch,
+                       cudaStream_t s, bool force_fp64) {
     switch (sdt) {
-        case IPFC_U8: return launch_out<uint8_t>(ddt, a, dkx, dky, scratch, s);
-        case IPFC_U16: return launch_out<uint16_t>(ddt, a, dkx, dky, scratch, s);
-        case IPFC_I16: return launch_out<int16_t>(ddt, a, dkx, dky, scratch, s);
-        case IPFC_F32: return launch_out<float>(ddt, a, dkx, dky, scratch, s);
+        case IPFC_U8: return launch_out<uint8_t>(ddt, a, dkx, dky, scratch, s, force_fp64);
+        case IPFC_U16: return launch_out<uint16_t>(ddt, a, dkx, dky, scratch, s, force_fp64);
+        case IPFC_I16: return launch_out<int16_t>(ddt, a, dkx, dky, scratch, s, force_fp64);
+        case IPFC_I32: return launch_out<int32_t>(ddt, a, dkx, dky, scratch, s, force_fp64);
+        case IPFC_F32: return launch_out<float>(ddt, a, dkx, dky, scratch, s, force_fp64);
+        case IPFC_F64: return launch_out<double>(ddt, a, dkx, dky, scratch, s, force_fp64);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -184,7 +227,7 @@ __global__ void __launch_bounds__(kThreads) box_kernel(const BoxArgs a, int TX, 
     const int q0 = blockIdx.x * TX;
     const int y0 = blockIdx.y * TY;
     load_tile<Tin, Tacc>(tin, RY, SW, a.src, a.spitch, a.W, a.H, a.C, q0 - a.ax * a.C, y0 - a.ay, a.border,
-                         static_cast<Tacc>(a.bv));
+                         std::is_same<Tacc, double>::value ? static_cast<Tacc>(a.bvd) : static_cast<Tacc>(a.bv));
     __syncthreads();
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int nt = blockDim.x * blockDim.y;
@@ -232,6 +275,9 @@ __global__ void __launch_bounds__(kThreads) box_kernel(const BoxArgs a, int TX, 
                 const float e = fmaf(fs, a.scale_hi, -p0);
                 out = static_cast<Tout>(p0 + fmaf(fs, a.scale_lo, e));
             }
+        } else if constexpr (std::is_same<Tacc, double>::value) {
+            // the reference's sum times fl64(1/(kw*kh)), one rounding
+            out = sat_from_d<Tout>(a.normalize ? __dmul_rn(S, a.scaled) : S);
         } else {
             const float v = a.normalize ? S * (a.scale_hi + a.scale_lo) : S;
             out = sat_from_f<Tout>(v);
@@ -267,13 +313,26 @@ cudaError_t box_out(int ddt, const BoxArgs& a, cudaStream_t s) {
         case IPFC_U16: return box_typed<Tin, uint16_t, Tacc>(a, s);
         case IPFC_I16: return box_typed<Tin, int16_t, Tacc>(a, s);
         case IPFC_F32: return box_typed<Tin, float, Tacc>(a, s);
+        case IPFC_I32: return box_typed<Tin, int32_t, double>(a, s);
+        case IPFC_F64: return box_typed<Tin, double, double>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 }  // namespace
 
-cudaError_t box_launch(int sdt, int ddt, const BoxArgs& a, bool exact_int, cudaStream_t s) {
+cudaError_t box_launch(int sdt, int ddt, const BoxArgs& a, bool exact_int, cudaStream_t s, bool force_fp64) {
+    if (force_fp64 || sep_wide(sdt, ddt)) {  // FP64 sums
+        switch (sdt) {
+            case IPFC_U8: return box_out<uint8_t, double>(ddt, a, s);
+            case IPFC_U16: return box_out<uint16_t, double>(ddt, a, s);
+            case IPFC_I16: return box_out<int16_t, double>(ddt, a, s);
+            case IPFC_I32: return box_out<int32_t, double>(ddt, a, s);
+            case IPFC_F32: return box_out<float, double>(ddt, a, s);
+            case IPFC_F64: return box_out<double, double>(ddt, a, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (sdt) {
         case IPFC_U8: return exact_int ? box_out<uint8_t, int>(ddt, a, s) : box_out<uint8_t, float>(ddt, a, s);
         case IPFC_U16: return exact_int ? box_out<uint16_t, int>(ddt, a, s) : box_out<uint16_t, float>(ddt, a, s);

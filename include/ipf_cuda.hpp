@@ -13,8 +13,10 @@
 // ipf::Error with the reference's "ipf: <function>: <reason>" text.  There
 // is no CPU fallback: without a usable GPU the calls throw.
 //
-// Element types provided: uint8, uint16, int16 and float (ImageU8, ImageU16,
-// ImageI16, ImageF); ImageI32 and ImageD throw ipf::Error.
+// Element types: all six of the reference (ImageU8, ImageU16, ImageI16,
+// ImageI32, ImageF, ImageD).  Calls with an int32 or double image on either
+// side accumulate in FP64 in the reference's own operation order, so their
+// results match ipf's bit for bit; the others accumulate in FP32.
 #pragma once
 
 #include <ipf/filter.hpp>

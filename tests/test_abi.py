@@ -80,10 +80,19 @@ def test_structuring_element_error():
         ipf.getStructuringElement(ipf.MorphShape.Rect, 0)
 
 
-def test_unsupported_dtype_is_reported_not_emulated():
-    with pytest.raises(ipf.Error) as e:
-        ipf.gaussianBlur(np.zeros((4, 4), np.float64), 1.0)
-    assert e.value.status == 5
+def test_unknown_dtype_code_is_rejected():
+    """Element codes outside the reference's six image types are refused
+    before any device work (IPFC_ERR_UNSUPPORTED)."""
+    import ctypes
+
+    from imageprocessingflex_b200 import _lib
+
+    lib = _lib.load()
+    x = np.zeros((4, 4), np.uint8)
+    sv = _lib.IpfcImage(x.ctypes.data, 4, 4, 1, 9, 4, 0)
+    dv = _lib.IpfcImage(x.ctypes.data, 4, 4, 1, 0, 4, 0)
+    assert lib.ipfc_gaussian_blur(ctypes.byref(sv), ctypes.byref(dv), 1.0, 0.0, 0, 3, None) == 5
+    assert b"element type" in lib.ipfc_last_error()
 
 
 def test_empty_image_returns_empty():

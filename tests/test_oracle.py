@@ -173,6 +173,83 @@ def test_restatement_matches_reference(orc, refimpl, shape):
                     np.testing.assert_array_equal(orc.dilate(img, se, it), refimpl.dilate(img, se, it))
 
 
+@pytest.mark.parametrize("shape", [(1, 1, 1), (11, 1, 3), (23, 17, 3), (40, 7, 4)], ids=lambda s: "x".join(map(str, s)))
+def test_restatement_matches_reference_int32_double(orc, refimpl, shape):
+    """The FP64-accumulated element types (ImageI32, ImageD, and TOut of those
+    types from uint8 sources): the restatement is bit-identical to the
+    reference for every op and border."""
+    w, h, c = shape
+    rng = np.random.default_rng(w * 17 + h + c)
+    for dt in (np.int32, np.float64, np.uint8):
+        img = oracle.random_image(w, h, c, dt, 3 * w + h + c)
+        if dt == np.int32:
+            img = (img.astype(np.int64) * 40000 - 5_000_000).astype(np.int32)  # beyond 2^24
+        outs = (None, np.float64, np.int32) if dt != np.uint8 else (np.float64, np.int32)
+        for b in oracle.BORDERS:
+            for kw, kh in ((3, 3), (5, 4), (1, 7)):
+                kx, ky = rng.normal(size=kw), rng.normal(size=kh)
+                for od in outs:
+                    np.testing.assert_array_equal(
+                        orc.sep_filter(img, kx, ky, border=b, delta=0.3, border_value=2.0, out_dtype=od),
+                        refimpl.sep_filter(img, kx, ky, border=b, delta=0.3, border_value=2.0, out_dtype=od))
+                k2 = rng.normal(size=(kh, kw)).astype(np.float32)
+                for od in outs:
+                    np.testing.assert_array_equal(orc.filter2d(img, k2, b, 0.5, (-1, -1), 7.0, od),
+                                                  refimpl.filter2d(img, k2, b, 0.5, (-1, -1), 7.0, od))
+                    for norm in (True, False):
+                        np.testing.assert_array_equal(orc.box_filter(img, kw, kh, norm, b, 3.0, od),
+                                                      refimpl.box_filter(img, kw, kh, norm, b, 3.0, od))
+            if b != CONSTANT and dt != np.uint8:
+                for k in (3, 5, 7):
+                    np.testing.assert_array_equal(orc.median_blur(img, k, b), refimpl.median_blur(img, k, b))
+        if dt != np.uint8:
+            for shp in (0, 1, 2):
+                se = orc.structuring_element(shp, 5, 3)
+                for it in (1, 2):
+                    np.testing.assert_array_equal(orc.erode(img, se, it), refimpl.erode(img, se, it))
+                    np.testing.assert_array_equal(orc.dilate(img, se, it), refimpl.dilate(img, se, it))
+
+
+@pytest.mark.parametrize("dt", [np.uint8, np.uint16, np.int16, np.int32, np.float32, np.float64],
+                         ids=lambda d: np.dtype(d).name)
+def test_restatement_matches_reference_callers(orc, refimpl, dt):
+    """morphologyEx, bilateralFilter, integralImage, adaptiveThreshold,
+    pyrDown / pyrUp, ssim, cornerHarris / cornerMinEigenVal and canny: the
+    restatement is bit-identical to the reference."""
+    rng = np.random.default_rng(5)
+    for (w, h, c) in ((1, 1, 1), (23, 17, 3), (40, 29, 1), (13, 31, 4)):
+        img = oracle.random_image(w, h, c, dt, w + h + c)
+        for op in range(7):
+            se = orc.structuring_element(op % 3, 5, 3)
+            for it in (1, 2):
+                np.testing.assert_array_equal(orc.morphology_ex(img, op, se, it), refimpl.morphology_ex(img, op, se, it))
+        for b in oracle.BORDERS:
+            for d, sc, ss in ((5, 30.0, 2.0), (0, 0.2, 1.4), (9, 75.0, 75.0)):
+                np.testing.assert_array_equal(orc.bilateral(img, d, sc, ss, b), refimpl.bilateral(img, d, sc, ss, b))
+        for sq in (False, True):
+            np.testing.assert_array_equal(orc.integral(img, sq), refimpl.integral(img, sq))
+        np.testing.assert_array_equal(orc.pyr_down(img), refimpl.pyr_down(img))
+        np.testing.assert_array_equal(orc.pyr_up(img), refimpl.pyr_up(img))
+        other = oracle.random_image(w, h, c, dt, 7 * w + h)
+        r1, m1 = orc.ssim(img, other, True)
+        r2, m2 = refimpl.ssim(img, other, True)
+        assert r1 == r2
+        np.testing.assert_array_equal(m1, m2)
+        for ks in (3, 5):
+            for l2 in (False, True):
+                lo, hi = (20.0, 60.0) if dt in (np.uint8, np.uint16, np.int16, np.int32) else (0.05, 0.3)
+                np.testing.assert_array_equal(orc.canny(img, lo, hi, ks, l2), refimpl.canny(img, lo, hi, ks, l2))
+        if c == 1:
+            for bs, ks in ((3, 3), (5, 5), (2, 1)):
+                for me in (False, True):
+                    np.testing.assert_array_equal(orc.corner(img, bs, ks, 0.04, me), refimpl.corner(img, bs, ks, 0.04, me))
+            for method in (0, 1):
+                for tt in (0, 1):
+                    for bs, cc in ((3, 2.0), (7, -1.5), (11, 0.0)):
+                        np.testing.assert_array_equal(orc.adaptive_threshold(img, 200.0, method, tt, bs, cc),
+                                                      refimpl.adaptive_threshold(img, 200.0, method, tt, bs, cc))
+
+
 def test_tap_generators_match_reference(orc, refimpl):
     for s in (0.3, 0.5, 1.0, 1.7, 2.0, 2.3, 4.0, 7.5):
         np.testing.assert_array_equal(orc.gaussian_kernel_1d(s), refimpl.gaussian_kernel_1d(s))
