@@ -6,11 +6,19 @@ tensors (device).  The C++ form is ``include/ipf_cuda.hpp``; the C ABI is
 ``include/ipfc.h``; the kernels live in ``csrc/``.
 """
 from .filters import (  # noqa: F401
+    AdaptiveMethod,
     BorderMode,
     Error,
+    MorphOp,
     MorphShape,
+    ThresholdType,
+    adaptiveThreshold,
+    bilateralFilter,
     blur,
     boxFilter,
+    canny,
+    cornerHarris,
+    cornerMinEigenVal,
     derivKernel,
     dilate,
     erode,
@@ -18,9 +26,14 @@ from .filters import (  # noqa: F401
     gaussianBlur,
     gaussianKernel1D,
     getStructuringElement,
+    integralImage,
     medianBlur,
+    morphologyEx,
+    pyrDown,
+    pyrUp,
     sepFilter2D,
     sobel,
+    ssim,
 )
 
 __version__ = "1.0.0"

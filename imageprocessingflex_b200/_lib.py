@@ -77,6 +77,16 @@ _SIGNATURES = {
     "ipfc_filter2d_noalloc": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_int, c_int, c_double,
                                       c_double, c_void_p]),
     "ipfc_median_blur": (c_int, [IMG_P, IMG_P, c_int, c_int, c_void_p]),
+    "ipfc_morphology_ex": (c_int, [IMG_P, IMG_P, c_int, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "ipfc_bilateral_filter": (c_int, [IMG_P, IMG_P, c_int, c_double, c_double, c_int, c_void_p]),
+    "ipfc_integral_image": (c_int, [IMG_P, IMG_P, c_int, c_void_p]),
+    "ipfc_adaptive_threshold": (c_int, [IMG_P, IMG_P, c_double, c_int, c_int, c_int, c_double, c_void_p]),
+    "ipfc_pyr_down": (c_int, [IMG_P, IMG_P, c_void_p]),
+    "ipfc_pyr_up": (c_int, [IMG_P, IMG_P, c_void_p]),
+    "ipfc_ssim": (c_int, [IMG_P, IMG_P, DBL_P, IMG_P, c_void_p]),
+    "ipfc_corner_harris": (c_int, [IMG_P, IMG_P, c_int, c_int, c_double, c_void_p]),
+    "ipfc_corner_min_eigen_val": (c_int, [IMG_P, IMG_P, c_int, c_int, c_void_p]),
+    "ipfc_canny": (c_int, [IMG_P, IMG_P, c_double, c_double, c_int, c_int, c_void_p]),
     "ipfc_erode": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_void_p]),
     "ipfc_dilate": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_void_p]),
     "ipfc_batch_create": (c_int, [c_void_p]),

@@ -38,6 +38,35 @@ class MorphShape(IntEnum):
     Ellipse = 2
 
 
+class MorphOp(IntEnum):
+    """ipf::MorphOp (morphology.hpp:129-138)."""
+
+    Erode = 0
+    Dilate = 1
+    Open = 2
+    Close = 3
+    Gradient = 4
+    TopHat = 5
+    BlackHat = 6
+
+
+class AdaptiveMethod(IntEnum):
+    """ipf::AdaptiveMethod (filter.hpp:545)."""
+
+    Mean = 0
+    Gaussian = 1
+
+
+class ThresholdType(IntEnum):
+    """ipf::ThresholdType (pixel_ops.hpp:253-259); adaptiveThreshold takes the first two."""
+
+    Binary = 0
+    BinaryInv = 1
+    Trunc = 2
+    ToZero = 3
+    ToZeroInv = 4
+
+
 class Error(RuntimeError):
     """ipf::Error (core.hpp:35-38): every failure is reported with this type."""
 
@@ -302,3 +331,138 @@ def erode(src, se=None, iterations=1, stream=None):
 def dilate(src, se=None, iterations=1, stream=None):
     """dilate (morphology.hpp:121-127); default element: 3x3 rect."""
     return _morph("ipfc_dilate", src, se, iterations, stream)
+
+
+def morphologyEx(src, op, se=None, iterations=1, stream=None):
+    """morphologyEx (morphology.hpp:140-158); default element: 3x3 rect."""
+    lib = _lib.load()
+    if se is None:
+        se = getStructuringElement(MorphShape.Rect, 3)
+    se = np.ascontiguousarray(np.asarray(se, dtype=np.uint8))
+    if se.ndim != 2 or se.size == 0:
+        raise Error("ipf: morphology: structuring element must be a non-empty single-channel mask")
+    sv, keep, dst, dv = _pair(src, None)
+    _check(lib.ipfc_morphology_ex(ctypes.byref(sv), ctypes.byref(dv), int(op), se.ctypes.data, se.shape[1],
+                                  se.shape[0], int(iterations), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def bilateralFilter(src, d, sigmaColor, sigmaSpace, border=BorderMode.Reflect101, stream=None):
+    """bilateralFilter (filter.hpp:337-387)."""
+    lib = _lib.load()
+    sv, keep, dst, dv = _pair(src, None)
+    _check(lib.ipfc_bilateral_filter(ctypes.byref(sv), ctypes.byref(dv), int(d), float(sigmaColor),
+                                     float(sigmaSpace), int(border), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def _alloc(src, shape, code):
+    """A destination of `shape` and element code in src's memory space: (obj, view)."""
+    if _is_tensor(src):
+        torch = _torch()
+        tmap = {U8: torch.uint8, U16: torch.uint16, I16: torch.int16, I32: torch.int32,
+                F32: torch.float32, F64: torch.float64}
+        dst = torch.empty(shape, dtype=tmap[code], device=src.device)
+        return dst, _view(dst)
+    dst = np.empty(shape, _CODE_NP[code])
+    dv, dst = _view(dst)
+    return dst, dv
+
+
+def _source(src):
+    if _is_tensor(src):
+        return _view(src), src
+    return _view(src)
+
+
+def integralImage(src, squared=False, stream=None):
+    """integralImage (filter.hpp:527-541): float64, (H+1) x (W+1) [x C]."""
+    lib = _lib.load()
+    sv, keep = _source(src)
+    w, h, c = _dims(src)
+    dst, dv = _alloc(src, (h + 1, w + 1) + ((c,) if src.ndim == 3 else ()), F64)
+    _check(lib.ipfc_integral_image(ctypes.byref(sv), ctypes.byref(dv), int(bool(squared)), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def adaptiveThreshold(src, maxval, method, type, blockSize, C, stream=None):
+    """adaptiveThreshold (filter.hpp:554-567), single channel."""
+    lib = _lib.load()
+    sv, keep, dst, dv = _pair(src, None)
+    _check(lib.ipfc_adaptive_threshold(ctypes.byref(sv), ctypes.byref(dv), float(maxval), int(method), int(type),
+                                       int(blockSize), float(C), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def pyrDown(src, stream=None):
+    """pyrDown (geometry.hpp:504-513): ((W+1)/2) x ((H+1)/2)."""
+    lib = _lib.load()
+    sv, keep = _source(src)
+    w, h, c = _dims(src)
+    dst, dv = _alloc(src, ((h + 1) // 2, (w + 1) // 2) + tuple(src.shape[2:]), sv.dtype)
+    _check(lib.ipfc_pyr_down(ctypes.byref(sv), ctypes.byref(dv), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def pyrUp(src, stream=None):
+    """pyrUp (geometry.hpp:516-525): 2W x 2H."""
+    lib = _lib.load()
+    sv, keep = _source(src)
+    w, h, c = _dims(src)
+    dst, dv = _alloc(src, (2 * h, 2 * w) + tuple(src.shape[2:]), sv.dtype)
+    _check(lib.ipfc_pyr_up(ctypes.byref(sv), ctypes.byref(dv), _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def ssim(a, b, ssimMap=False, stream=None):
+    """ssim (metrics.hpp:51-78): the mean SSIM, and with ssimMap=True also the
+    float32 per-pixel map (the reference's ImageF* out-parameter)."""
+    lib = _lib.load()
+    av, keep_a = _source(a)
+    bv, keep_b = _source(b)
+    res = ctypes.c_double(0.0)
+    m = mv = None
+    if ssimMap:
+        m, mv = _alloc(a, tuple(a.shape), F32)
+    _check(lib.ipfc_ssim(ctypes.byref(av), ctypes.byref(bv), ctypes.byref(res),
+                         ctypes.byref(mv) if ssimMap else None, _stream_of(a, stream)))
+    del keep_a, keep_b
+    return (res.value, m) if ssimMap else res.value
+
+
+def _corners(fn, src, args, stream):
+    lib = _lib.load()
+    sv, keep = _source(src)
+    w, h, c = _dims(src)
+    dst, dv = _alloc(src, (h, w), F32)
+    _check(getattr(lib, fn)(ctypes.byref(sv), ctypes.byref(dv), *args, _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def cornerHarris(src, blockSize=3, ksize=3, k=0.04, stream=None):
+    """cornerHarris (features.hpp:128-136): float32 response."""
+    return _corners("ipfc_corner_harris", src, (int(blockSize), int(ksize), float(k)), stream)
+
+
+def cornerMinEigenVal(src, blockSize=3, ksize=3, stream=None):
+    """cornerMinEigenVal (features.hpp:138-146): float32 response."""
+    return _corners("ipfc_corner_min_eigen_val", src, (int(blockSize), int(ksize)), stream)
+
+
+def canny(src, lowThreshold, highThreshold, ksize=3, l2Gradient=False, stream=None):
+    """canny (features.hpp:27-88): uint8 0/255 edge map, single channel."""
+    lib = _lib.load()
+    sv, keep = _source(src)
+    w, h, c = _dims(src)
+    dst, dv = _alloc(src, (h, w), U8)
+    _check(lib.ipfc_canny(ctypes.byref(sv), ctypes.byref(dv), float(lowThreshold), float(highThreshold), int(ksize),
+                          int(bool(l2Gradient)), _stream_of(src, stream)))
+    del keep
+    return dst

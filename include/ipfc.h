@@ -198,6 +198,74 @@ IPFC_API int ipfc_erode(const ipfc_image* src, ipfc_image* dst, const uint8_t* s
 IPFC_API int ipfc_dilate(const ipfc_image* src, ipfc_image* dst, const uint8_t* se, int se_w, int se_h, int iterations,
                 void* stream);
 
+/* morphologyEx (morphology.hpp:140-158): op in ipf::MorphOp order; the
+ * compound ops run the same erode / dilate kernels through device buffers,
+ * and differences are saturate_cast<T>(double(a) - double(b)). */
+enum {
+    IPFC_MORPH_ERODE = 0,
+    IPFC_MORPH_DILATE = 1,
+    IPFC_MORPH_OPEN = 2,
+    IPFC_MORPH_CLOSE = 3,
+    IPFC_MORPH_GRADIENT = 4,
+    IPFC_MORPH_TOPHAT = 5,
+    IPFC_MORPH_BLACKHAT = 6
+};
+IPFC_API int ipfc_morphology_ex(const ipfc_image* src, ipfc_image* dst, int op, const uint8_t* se, int se_w, int se_h,
+                                int iterations, void* stream);
+
+/* ---- more filters and the reference's callers of the filters ---------------
+ *
+ * Each is computed on the GPU with the kernels above; where the reference
+ * accumulates in FP64 these do too, in its operation order, so results are
+ * bit-identical to ipf's unless noted. */
+
+/* bilateralFilter (filter.hpp:337-387): circular window of radius d/2 (or
+ * lround(1.5 sigma_space) for d <= 0, at most 64), L1 colour distance,
+ * Constant-border positions skipped.  Integer images use the reference's
+ * range-weight table (bit-identical); float images evaluate exp per tap on
+ * the GPU (within a few units in the last place of FP64).  1 to 4 channels. */
+IPFC_API int ipfc_bilateral_filter(const ipfc_image* src, ipfc_image* dst, int d, double sigma_color,
+                                   double sigma_space, int border, void* stream);
+
+/* integralImage (filter.hpp:527-541): dst is IPFC_F64 with (W+1) x (H+1)
+ * pixels and the source's channels; squared != 0 sums squares. */
+IPFC_API int ipfc_integral_image(const ipfc_image* src, ipfc_image* dst, int squared, void* stream);
+
+/* adaptiveThreshold (filter.hpp:554-567): single channel; method and type in
+ * ipf's AdaptiveMethod / ThresholdType order (Binary and BinaryInv only). */
+enum { IPFC_ADAPTIVE_MEAN = 0, IPFC_ADAPTIVE_GAUSSIAN = 1 };
+enum { IPFC_THRESH_BINARY = 0, IPFC_THRESH_BINARY_INV = 1 };
+IPFC_API int ipfc_adaptive_threshold(const ipfc_image* src, ipfc_image* dst, double maxval, int method, int type,
+                                     int block_size, double c, void* stream);
+
+/* pyrDown / pyrUp (geometry.hpp:504-525): dst is ((W+1)/2) x ((H+1)/2),
+ * respectively 2W x 2H, same type and channels. */
+IPFC_API int ipfc_pyr_down(const ipfc_image* src, ipfc_image* dst, void* stream);
+IPFC_API int ipfc_pyr_up(const ipfc_image* src, ipfc_image* dst, void* stream);
+
+/* ssim (metrics.hpp:51-78): mean SSIM of a and b (same shape and type) over
+ * the valid region into *result; ssim_map (nullable) receives the per-pixel
+ * map, IPFC_F32 with a's shape.  The map is bit-identical to the reference's;
+ * the mean is a parallel FP64 sum (within 1e-12 relative of its sequential
+ * one). */
+IPFC_API int ipfc_ssim(const ipfc_image* a, const ipfc_image* b, double* result, ipfc_image* ssim_map, void* stream);
+
+/* cornerHarris / cornerMinEigenVal (features.hpp:111-142): single-channel
+ * source, dst IPFC_F32.  The Sobel terms are bit-identical; the unnormalised
+ * box sums are FP64 window sums where the reference keeps FP64 running sums,
+ * so results agree to about one unit in the last place of FP32. */
+IPFC_API int ipfc_corner_harris(const ipfc_image* src, ipfc_image* dst, int block_size, int ksize, double k,
+                                void* stream);
+IPFC_API int ipfc_corner_min_eigen_val(const ipfc_image* src, ipfc_image* dst, int block_size, int ksize,
+                                       void* stream);
+
+/* canny (features.hpp:27-88): dst is IPFC_U8, single channel, 0 / 255.  Sobel
+ * gradients with Replicate, per-pixel strongest channel, non-maximum
+ * suppression and hysteresis (propagated on the GPU until no edge changes;
+ * the result does not depend on the visiting order). */
+IPFC_API int ipfc_canny(const ipfc_image* src, ipfc_image* dst, double low_threshold, double high_threshold, int ksize,
+                        int l2_gradient, void* stream);
+
 /* ---- batches: many images, a few launches --------------------------------
  *
  * No counterpart in the reference (ipf runs one call per image).  A batch

@@ -176,6 +176,95 @@ class CpuFilters:
             raise ValueError(f"ipf: filter2D failed ({rcs})")
         return out
 
+    # -- the reference's other filters and callers of the filters -------------
+    def morphology_ex(self, src, op, se, iterations=1):
+        src = np.ascontiguousarray(src)
+        se = np.ascontiguousarray(se, np.uint8)
+        out = np.zeros_like(src)
+        W, H, C = _shape(src)
+        rc = self._f("morphology_ex")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out), op, _ptr(se),
+                                      se.shape[1], se.shape[0], iterations)
+        if rc:
+            raise ValueError(f"ipf: morphologyEx failed ({rc})")
+        return out
+
+    def bilateral(self, src, d, sigma_color, sigma_space, border=REFLECT101):
+        src = np.ascontiguousarray(src)
+        out = np.zeros_like(src)
+        W, H, C = _shape(src)
+        rc = self._f("bilateral")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out), d, _c_double(sigma_color),
+                                  _c_double(sigma_space), border)
+        if rc:
+            raise ValueError(f"ipf: bilateralFilter failed ({rc})")
+        return out
+
+    def integral(self, src, squared=False):
+        src = np.ascontiguousarray(src)
+        W, H, C = _shape(src)
+        out = np.zeros((H + 1, W + 1) + ((C,) if src.ndim == 3 else ()), np.float64)
+        rc = self._f("integral")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out), int(bool(squared)))
+        if rc:
+            raise ValueError(f"ipf: integralImage failed ({rc})")
+        return out
+
+    def adaptive_threshold(self, src, maxval, method, ttype, block_size, c):
+        src = np.ascontiguousarray(src)
+        out = np.zeros_like(src)
+        W, H, _ = _shape(src)
+        rc = self._f("adaptive_threshold")(_ptr(src), DTYPE_CODE[src.dtype], W, H, _ptr(out), _c_double(maxval),
+                                           method, ttype, block_size, _c_double(c))
+        if rc:
+            raise ValueError(f"ipf: adaptiveThreshold failed ({rc})")
+        return out
+
+    def pyr_down(self, src):
+        src = np.ascontiguousarray(src)
+        W, H, C = _shape(src)
+        out = np.zeros(((H + 1) // 2, (W + 1) // 2) + src.shape[2:], src.dtype)
+        if self._f("pyr_down")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out)):
+            raise ValueError("ipf: pyrDown failed")
+        return out
+
+    def pyr_up(self, src):
+        src = np.ascontiguousarray(src)
+        W, H, C = _shape(src)
+        out = np.zeros((2 * H, 2 * W) + src.shape[2:], src.dtype)
+        if self._f("pyr_up")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out)):
+            raise ValueError("ipf: pyrUp failed")
+        return out
+
+    def ssim(self, a, b, want_map=False):
+        a = np.ascontiguousarray(a)
+        b = np.ascontiguousarray(b)
+        W, H, C = _shape(a)
+        res = np.zeros(1, np.float64)
+        m = np.zeros(a.shape, np.float32) if want_map else None
+        rc = self._f("ssim")(_ptr(a), _ptr(b), DTYPE_CODE[a.dtype], W, H, C, _ptr(res),
+                             _ptr(m) if want_map else None)
+        if rc:
+            raise ValueError(f"ipf: ssim failed ({rc})")
+        return (float(res[0]), m) if want_map else float(res[0])
+
+    def corner(self, src, block_size=3, ksize=3, k=0.04, min_eig=False):
+        src = np.ascontiguousarray(src)
+        W, H, _ = _shape(src)
+        out = np.zeros((H, W), np.float32)
+        rc = self._f("corner")(_ptr(src), DTYPE_CODE[src.dtype], W, H, _ptr(out), block_size, ksize, _c_double(k),
+                               int(bool(min_eig)))
+        if rc:
+            raise ValueError(f"ipf: corner response failed ({rc})")
+        return out
+
+    def canny(self, src, low, high, ksize=3, l2=False):
+        src = np.ascontiguousarray(src)
+        W, H, C = _shape(src)
+        out = np.zeros((H, W), np.uint8)
+        rc = self._f("canny")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out), _c_double(low),
+                              _c_double(high), ksize, int(bool(l2)))
+        if rc:
+            raise ValueError(f"ipf: canny failed ({rc})")
+        return out
+
     def box_filter(self, src, kw, kh, normalize=True, border=REFLECT101, border_value=0.0, out_dtype=None):
         src = np.ascontiguousarray(src)
         out = self._out(src, out_dtype)

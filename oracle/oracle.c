@@ -508,3 +508,388 @@ int orc_morph(const void* src, int dt, int W, int H, int C, void* dst, const uin
     free(a); free(b); free(t);
     return ORC_OK;
 }
+
+/* ===========================================================================
+ * The reference's other filters and the callers of the filters.
+ * ======================================================================== */
+
+/* ipf::PixelTraits<T>::max() (core.hpp:53-66). */
+static double pixel_max(int dt) {
+    switch (dt) {
+        case ORC_U8: return 255.0;
+        case ORC_U16: return 65535.0;
+        case ORC_I16: return 32767.0;
+        case ORC_I32: return 255.0;
+        default: return 1.0;
+    }
+}
+
+/* morphology.hpp:140-158 (morphologyEx): op 0 Erode, 1 Dilate, 2 Open,
+ * 3 Close, 4 Gradient, 5 TopHat, 6 BlackHat; differences are
+ * saturate_cast<T>(double(a) - double(b)). */
+int orc_morphology_ex(const void* src, int dt, int W, int H, int C, void* dst, int op, const uint8_t* se, int sw,
+                      int sh, int iterations) {
+    if (op < 0 || op > 6) return ORC_EINVAL;
+    if (op == 0) return orc_morph(src, dt, W, H, C, dst, se, sw, sh, 1, iterations);
+    if (op == 1) return orc_morph(src, dt, W, H, C, dst, se, sw, sh, 0, iterations);
+    const size_t n = (size_t)W * H * C, es = elem_size(dt);
+    void* t1 = malloc(n * es + 1);
+    void* t2 = malloc(n * es + 1);
+    if (!t1 || !t2) {
+        free(t1); free(t2);
+        return ORC_ENOMEM;
+    }
+    int rc = ORC_OK;
+    const void *a = NULL, *b = NULL;
+    switch (op) {
+        case 2:  /* dilate(erode(x)) */
+            rc = orc_morph(src, dt, W, H, C, t1, se, sw, sh, 1, iterations);
+            if (!rc) rc = orc_morph(t1, dt, W, H, C, dst, se, sw, sh, 0, iterations);
+            break;
+        case 3:  /* erode(dilate(x)) */
+            rc = orc_morph(src, dt, W, H, C, t1, se, sw, sh, 0, iterations);
+            if (!rc) rc = orc_morph(t1, dt, W, H, C, dst, se, sw, sh, 1, iterations);
+            break;
+        case 4:  /* dilate(x) - erode(x) */
+            rc = orc_morph(src, dt, W, H, C, t1, se, sw, sh, 0, iterations);
+            if (!rc) rc = orc_morph(src, dt, W, H, C, t2, se, sw, sh, 1, iterations);
+            a = t1; b = t2;
+            break;
+        case 5:  /* x - open(x) */
+            rc = orc_morph(src, dt, W, H, C, t1, se, sw, sh, 1, iterations);
+            if (!rc) rc = orc_morph(t1, dt, W, H, C, t2, se, sw, sh, 0, iterations);
+            a = src; b = t2;
+            break;
+        default: /* close(x) - x */
+            rc = orc_morph(src, dt, W, H, C, t1, se, sw, sh, 0, iterations);
+            if (!rc) rc = orc_morph(t1, dt, W, H, C, t2, se, sw, sh, 1, iterations);
+            a = t2; b = src;
+            break;
+    }
+    if (!rc && a)
+        for (size_t i = 0; i < n; ++i) store_sat(dst, dt, i, load_elem(a, dt, i) - load_elem(b, dt, i));
+    free(t1); free(t2);
+    return rc;
+}
+
+/* filter.hpp:337-387 (bilateralFilter): circular window of radius d/2 (or
+ * lround(1.5 sigmaSpace)), spatial Gaussian, range Gaussian of the L1 colour
+ * distance (table by integer distance for integer images), Constant-border
+ * positions skipped, FP64 throughout. */
+int orc_bilateral(const void* src, int dt, int W, int H, int C, void* dst, int d, double sigma_color,
+                  double sigma_space, int border) {
+    if (!(sigma_color > 0 && sigma_space > 0)) return ORC_EINVAL;
+    if (W <= 0 || H <= 0) return ORC_OK;
+    const int r = d <= 0 ? (int)lround(sigma_space * 1.5) : d / 2;
+    int nt = 0;
+    int* tdx = (int*)malloc(sizeof(int) * (size_t)(2 * r + 1) * (2 * r + 1));
+    int* tdy = (int*)malloc(sizeof(int) * (size_t)(2 * r + 1) * (2 * r + 1));
+    double* tw = (double*)malloc(sizeof(double) * (size_t)(2 * r + 1) * (2 * r + 1));
+    int* xt = border_table(W, r, r, border);
+    int* yt = border_table(H, r, r, border);
+    double* lut = NULL;
+    size_t nlut = 0;
+    const double cc = -1.0 / (2 * sigma_color * sigma_color);
+    if (dt != ORC_F32 && dt != ORC_F64) {
+        const double max_dist = pixel_max(dt) * C;
+        if (max_dist <= (1 << 20)) {
+            nlut = (size_t)max_dist + 1;
+            lut = (double*)malloc(sizeof(double) * nlut);
+            if (lut)
+                for (size_t k = 0; k < nlut; ++k) lut[k] = exp((double)(k * k) * cc);
+        }
+    }
+    double* acc = (double*)malloc(sizeof(double) * (size_t)C);
+    if (!tdx || !tdy || !tw || !xt || !yt || !acc || (nlut && !lut)) {
+        free(tdx); free(tdy); free(tw); free(xt); free(yt); free(lut); free(acc);
+        return ORC_ENOMEM;
+    }
+    for (int j = -r; j <= r; ++j)
+        for (int i = -r; i <= r; ++i)
+            if (i * i + j * j <= r * r) {
+                tdx[nt] = i;
+                tdy[nt] = j;
+                tw[nt] = exp(-(i * i + j * j) / (2 * sigma_space * sigma_space));
+                ++nt;
+            }
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const size_t p0 = ((size_t)y * W + x) * C;
+            for (int c = 0; c < C; ++c) acc[c] = 0.0;
+            double wsum = 0;
+            for (int t = 0; t < nt; ++t) {
+                const int sx = xt[x + r + tdx[t]], sy = yt[y + r + tdy[t]];
+                if (sx < 0 || sy < 0) continue;
+                const size_t p = ((size_t)sy * W + sx) * C;
+                double dist = 0;
+                for (int c = 0; c < C; ++c) dist += fabs(load_elem(src, dt, p + c) - load_elem(src, dt, p0 + c));
+                const double w = tw[t] * (lut ? lut[(size_t)dist] : exp(dist * dist * cc));
+                wsum += w;
+                for (int c = 0; c < C; ++c) acc[c] += w * load_elem(src, dt, p + c);
+            }
+            for (int c = 0; c < C; ++c) store_sat(dst, dt, p0 + c, acc[c] / wsum);
+        }
+    free(tdx); free(tdy); free(tw); free(xt); free(yt); free(lut); free(acc);
+    return ORC_OK;
+}
+
+/* filter.hpp:527-541 (integralImage): I is (W+1) x (H+1) x C doubles,
+ * I(x+1, y+1) = I(x+1, y) + (running row sum of row y up to x). */
+int orc_integral(const void* src, int dt, int W, int H, int C, double* I, int squared) {
+    const size_t iw = (size_t)(W + 1) * C;
+    for (size_t i = 0; i < iw * (size_t)(H + 1); ++i) I[i] = 0.0;
+    double* rs = (double*)malloc(sizeof(double) * (size_t)(C > 0 ? C : 1));
+    if (!rs) return ORC_ENOMEM;
+    for (int y = 0; y < H; ++y) {
+        for (int c = 0; c < C; ++c) rs[c] = 0.0;
+        for (int x = 0; x < W; ++x)
+            for (int c = 0; c < C; ++c) {
+                const double v = load_elem(src, dt, ((size_t)y * W + x) * C + c);
+                rs[c] += squared ? v * v : v;
+                I[(size_t)(y + 1) * iw + (size_t)(x + 1) * C + c] = I[(size_t)y * iw + (size_t)(x + 1) * C + c] + rs[c];
+            }
+    }
+    free(rs);
+    return ORC_OK;
+}
+
+/* filter.hpp:554-567 (adaptiveThreshold), single channel: the local mean by
+ * boxFilter (method 0) or gaussianBlur (method 1) with Replicate, in the
+ * source's type; type 0 Binary, 1 BinaryInv. */
+int orc_adaptive_threshold(const void* src, int dt, int W, int H, void* dst, double maxval, int method, int type,
+                           int bs, double c) {
+    if (bs < 3 || bs % 2 != 1 || (type != 0 && type != 1)) return ORC_EINVAL;
+    if (W <= 0 || H <= 0) return ORC_OK;
+    const size_t n = (size_t)W * H;
+    void* mean = malloc(n * elem_size(dt) + 1);
+    if (!mean) return ORC_ENOMEM;
+    int rc;
+    if (method == 0) {
+        rc = orc_box_filter(src, dt, W, H, 1, mean, dt, bs, bs, 1, ORC_REPLICATE, 0.0);
+    } else {
+        double k[64];
+        const int kl = orc_gaussian_kernel_1d(0.0, bs, k, 64);
+        rc = kl < 0 || kl > 64 ? ORC_EINVAL
+                                : orc_sep_filter(src, dt, W, H, 1, mean, dt, k, kl, k, kl, kl / 2, kl / 2,
+                                                 ORC_REPLICATE, 0.0, 0.0);
+    }
+    if (!rc)
+        for (size_t i = 0; i < n; ++i) {
+            const int above = load_elem(src, dt, i) - load_elem(mean, dt, i) > -c;
+            store_sat(dst, dt, i, (above == (type == 0)) ? maxval : 0.0);
+        }
+    free(mean);
+    return rc;
+}
+
+/* geometry.hpp:504-513 (pyrDown): sepFilter2D<double> with the 5-tap binomial
+ * / 16 (Reflect101), every other row and column, saturate_cast. */
+int orc_pyr_down(const void* src, int dt, int W, int H, int C, void* dst) {
+    if (W <= 0 || H <= 0) return ORC_OK;
+    const double k[5] = {1 / 16.0, 4 / 16.0, 6 / 16.0, 4 / 16.0, 1 / 16.0};
+    double* b = (double*)malloc(sizeof(double) * (size_t)W * H * C);
+    if (!b) return ORC_ENOMEM;
+    int rc = orc_sep_filter(src, dt, W, H, C, b, ORC_F64, k, 5, k, 5, 2, 2, ORC_REFLECT101, 0.0, 0.0);
+    const int W2 = (W + 1) / 2, H2 = (H + 1) / 2;
+    if (!rc)
+        for (int y = 0; y < H2; ++y)
+            for (int x = 0; x < W2; ++x)
+                for (int c = 0; c < C; ++c)
+                    store_sat(dst, dt, ((size_t)y * W2 + x) * C + c, b[((size_t)(2 * y) * W + 2 * x) * C + c]);
+    free(b);
+    return rc;
+}
+
+/* geometry.hpp:516-525 (pyrUp): zero insertion into a double image of twice
+ * the size, then sepFilter2D<T> with the binomial / 8 (Reflect101). */
+int orc_pyr_up(const void* src, int dt, int W, int H, int C, void* dst) {
+    if (W <= 0 || H <= 0) return ORC_OK;
+    const int W2 = 2 * W, H2 = 2 * H;
+    double* up = (double*)calloc((size_t)W2 * H2 * C, sizeof(double));
+    if (!up) return ORC_ENOMEM;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+            for (int c = 0; c < C; ++c)
+                up[((size_t)(2 * y) * W2 + 2 * x) * C + c] = load_elem(src, dt, ((size_t)y * W + x) * C + c);
+    const double k[5] = {1 / 8.0, 4 / 8.0, 6 / 8.0, 4 / 8.0, 1 / 8.0};
+    const int rc = orc_sep_filter(up, ORC_F64, W2, H2, C, dst, dt, k, 5, k, 5, 2, 2, ORC_REFLECT101, 0.0, 0.0);
+    free(up);
+    return rc;
+}
+
+/* metrics.hpp:51-78 (ssim): 11-tap Gaussian (sigma 1.5, Reflect101) means of
+ * x, y, x^2, y^2, xy in FP64; the map in float; the mean over the valid
+ * region (5-pixel margin when the image is larger than 10 x 10). */
+int orc_ssim(const void* a, const void* b, int dt, int W, int H, int C, double* result, float* map) {
+    if (W <= 0 || H <= 0) return ORC_EINVAL;
+    const size_t n = (size_t)W * H * C;
+    const double L = pixel_max(dt), C1 = (0.01 * L) * (0.01 * L), C2 = (0.03 * L) * (0.03 * L);
+    double* buf = (double*)malloc(sizeof(double) * n * 10);
+    float* mp = map ? map : (float*)malloc(sizeof(float) * n);
+    if (!buf || !mp) {
+        free(buf);
+        if (!map) free(mp);
+        return ORC_ENOMEM;
+    }
+    double *x = buf, *y = buf + n, *xx = buf + 2 * n, *yy = buf + 3 * n, *xy = buf + 4 * n;
+    double *mx = buf + 5 * n, *my = buf + 6 * n, *sxx = buf + 7 * n, *syy = buf + 8 * n, *sxy = buf + 9 * n;
+    for (size_t i = 0; i < n; ++i) {
+        x[i] = load_elem(a, dt, i);
+        y[i] = load_elem(b, dt, i);
+        xx[i] = x[i] * x[i];
+        yy[i] = y[i] * y[i];
+        xy[i] = x[i] * y[i];
+    }
+    double g[16];
+    const int gl = orc_gaussian_kernel_1d(1.5, 11, g, 16);
+    double* ins[5] = {x, y, xx, yy, xy};
+    double* outs[5] = {mx, my, sxx, syy, sxy};
+    int rc = ORC_OK;
+    for (int i = 0; i < 5 && !rc; ++i)
+        rc = orc_sep_filter(ins[i], ORC_F64, W, H, C, outs[i], ORC_F64, g, gl, g, gl, gl / 2, gl / 2, ORC_REFLECT101,
+                            0.0, 0.0);
+    if (!rc) {
+        for (size_t i = 0; i < n; ++i) {
+            const double ux = mx[i], uy = my[i];
+            const double vx = sxx[i] - ux * ux, vy = syy[i] - uy * uy, cxy = sxy[i] - ux * uy;
+            mp[i] = (float)(((2 * ux * uy + C1) * (2 * cxy + C2)) / ((ux * ux + uy * uy + C1) * (vx + vy + C2)));
+        }
+        const int r = 5;
+        const int valid = W > 2 * r && H > 2 * r;
+        const int rx = valid ? r : 0, ry = valid ? r : 0, rw = valid ? W - 2 * r : W, rh = valid ? H - 2 * r : H;
+        double s = 0;
+        for (int yy0 = ry; yy0 < ry + rh; ++yy0)
+            for (int xx0 = rx; xx0 < rx + rw; ++xx0)
+                for (int c = 0; c < C; ++c) s += mp[((size_t)yy0 * W + xx0) * C + c];
+        *result = s / ((double)rw * rh * C);
+    }
+    free(buf);
+    if (!map) free(mp);
+    return rc;
+}
+
+/* Sobel of order (dx, dy) into float (filter.hpp:395-407): derivKernel taps,
+ * ksize 1 kept 3 long, `scale` folded into the horizontal taps. */
+static int sobel_f32(const void* src, int dt, int W, int H, int C, float* out, int dx, int dy, int ksize,
+                     double scale, int border) {
+    double kx[32], ky[32];
+    int nx = orc_deriv_kernel(dx, ksize, kx, 32), ny = orc_deriv_kernel(dy, ksize, ky, 32);
+    if (nx < 0 || ny < 0) return ORC_EINVAL;
+    if (ksize == 1) {
+        if (nx == 1) { kx[0] = 0; kx[1] = 1; kx[2] = 0; nx = 3; }
+        if (ny == 1) { ky[0] = 0; ky[1] = 1; ky[2] = 0; ny = 3; }
+    }
+    for (int i = 0; i < nx; ++i) kx[i] *= scale;
+    return orc_sep_filter(src, dt, W, H, C, out, ORC_F32, kx, nx, ky, ny, nx / 2, ny / 2, border, 0.0, 0.0);
+}
+
+/* features.hpp:111-142 (detail::structureTensor, cornerHarris,
+ * cornerMinEigenVal): single channel, float response. */
+int orc_corner(const void* src, int dt, int W, int H, float* dst, int bs, int ksize, double k, int min_eig) {
+    if (W <= 0 || H <= 0) return ORC_OK;
+    double scale = (double)(1 << ((ksize > 0 ? ksize : 3) - 1)) * bs;
+    if (dt != ORC_F32 && dt != ORC_F64) scale *= pixel_max(dt);
+    scale = 1.0 / scale;
+    const size_t n = (size_t)W * H;
+    float* f = (float*)malloc(sizeof(float) * n * 8);
+    if (!f) return ORC_ENOMEM;
+    float *gx = f, *gy = f + n, *xx = f + 2 * n, *xy = f + 3 * n, *yy = f + 4 * n, *ra = f + 5 * n, *rb = f + 6 * n,
+          *rc_ = f + 7 * n;
+    int rc = sobel_f32(src, dt, W, H, 1, gx, 1, 0, ksize, scale, ORC_REFLECT101);
+    if (!rc) rc = sobel_f32(src, dt, W, H, 1, gy, 0, 1, ksize, scale, ORC_REFLECT101);
+    if (!rc) {
+        for (size_t i = 0; i < n; ++i) {
+            xx[i] = gx[i] * gx[i];
+            xy[i] = gx[i] * gy[i];
+            yy[i] = gy[i] * gy[i];
+        }
+        rc = orc_box_filter(xx, ORC_F32, W, H, 1, ra, ORC_F32, bs, bs, 0, ORC_REFLECT101, 0.0);
+        if (!rc) rc = orc_box_filter(xy, ORC_F32, W, H, 1, rb, ORC_F32, bs, bs, 0, ORC_REFLECT101, 0.0);
+        if (!rc) rc = orc_box_filter(yy, ORC_F32, W, H, 1, rc_, ORC_F32, bs, bs, 0, ORC_REFLECT101, 0.0);
+    }
+    if (!rc)
+        for (size_t i = 0; i < n; ++i) {
+            if (min_eig) {
+                const double A = ra[i] * 0.5, B = rb[i], C = rc_[i] * 0.5;
+                dst[i] = (float)((A + C) - sqrt((A - C) * (A - C) + B * B));
+            } else {
+                const double A = ra[i], B = rb[i], C = rc_[i];
+                dst[i] = (float)(A * C - B * B - k * (A + C) * (A + C));
+            }
+        }
+    free(f);
+    return rc;
+}
+
+/* features.hpp:27-88 (canny): Sobel gradients (Replicate), the strongest
+ * channel per pixel, non-maximum suppression, hysteresis by a worklist. */
+int orc_canny(const void* src, int dt, int W, int H, int C, uint8_t* dst, double low, double high, int ksize, int l2) {
+    if (!(low <= high)) return ORC_EINVAL;
+    if (W <= 0 || H <= 0) return ORC_OK;
+    const size_t n = (size_t)W * H;
+    float* f = (float*)malloc(sizeof(float) * n * (2 * (size_t)C + 3));
+    int* q = (int*)malloc(sizeof(int) * n);
+    if (!f || !q) {
+        free(f); free(q);
+        return ORC_ENOMEM;
+    }
+    float *gx = f, *gy = f + n * C, *mag = f + 2 * n * C, *dx = mag + n, *dy = dx + n;
+    int rc = sobel_f32(src, dt, W, H, C, gx, 1, 0, ksize, 1.0, ORC_REPLICATE);
+    if (!rc) rc = sobel_f32(src, dt, W, H, C, gy, 0, 1, ksize, 1.0, ORC_REPLICATE);
+    if (rc) {
+        free(f); free(q);
+        return rc;
+    }
+    for (size_t i = 0; i < n; ++i) {
+        float best = -1;
+        for (int c = 0; c < C; ++c) {
+            const float a = gx[i * C + c], b = gy[i * C + c];
+            const float m = l2 ? sqrtf(a * a + b * b) : fabsf(a) + fabsf(b);
+            if (m > best) {
+                best = m;
+                dx[i] = a;
+                dy[i] = b;
+            }
+        }
+        mag[i] = best;
+    }
+    memset(dst, 0, n);
+    const float tan22 = 0.41421356f;
+#define ORC_M(X, Y) (((X) < 0 || (Y) < 0 || (X) >= W || (Y) >= H) ? 0.f : mag[(size_t)(Y) * W + (X)])
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const size_t i = (size_t)y * W + x;
+            const float m = mag[i];
+            if (m <= low) continue;
+            const float ax = fabsf(dx[i]), ay = fabsf(dy[i]);
+            int is_max;
+            if (ay <= ax * tan22) {
+                is_max = m > ORC_M(x - 1, y) && m >= ORC_M(x + 1, y);
+            } else if (ay * tan22 >= ax) {
+                is_max = m > ORC_M(x, y - 1) && m >= ORC_M(x, y + 1);
+            } else {
+                const int s = (dx[i] < 0) != (dy[i] < 0) ? -1 : 1;
+                is_max = m > ORC_M(x - s, y - 1) && m > ORC_M(x + s, y + 1);
+            }
+            if (is_max) dst[i] = m > high ? 2 : 1;
+        }
+#undef ORC_M
+    size_t head = 0, tail = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (dst[i] == 2) q[tail++] = (int)i;
+    while (head < tail) {
+        const int p = q[head++], px = p % W, py = p / W;
+        for (int j = -1; j <= 1; ++j)
+            for (int i = -1; i <= 1; ++i) {
+                const int nx = px + i, ny = py + j;
+                if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;
+                uint8_t* s = &dst[(size_t)ny * W + nx];
+                if (*s != 1) continue;
+                *s = 2;
+                q[tail++] = ny * W + nx;
+            }
+    }
+    for (size_t i = 0; i < n; ++i) dst[i] = dst[i] == 2 ? 255 : 0;
+    free(f); free(q);
+    return ORC_OK;
+}

@@ -9,7 +9,10 @@
 //
 // Signatures mirror oracle.c's orc_* functions with a ref_ prefix; element and
 // border codes are the same.
+#include <ipf/features.hpp>
 #include <ipf/filter.hpp>
+#include <ipf/geometry.hpp>
+#include <ipf/metrics.hpp>
 #include <ipf/morphology.hpp>
 
 #include <cstdint>
@@ -187,6 +190,105 @@ int ref_morph(const void* src, int dt, int W, int H, int C, void* dst, const std
             using S = decltype(s);
             const Image<S> in = wrap<S>(src, W, H, C);
             unwrap(is_erode ? ipf::erode(in, el, iterations) : ipf::dilate(in, el, iterations), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_morphology_ex(const void* src, int dt, int W, int H, int C, void* dst, int op, const std::uint8_t* se, int sw,
+                      int sh, int iterations) {
+    return guard([&] {
+        const StructuringElement el = StructuringElement::fromData(sw, sh, 1, se);
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::morphologyEx(wrap<S>(src, W, H, C), static_cast<MorphOp>(op), el, iterations), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_bilateral(const void* src, int dt, int W, int H, int C, void* dst, int d, double sc, double ss, int border) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::bilateralFilter(wrap<S>(src, W, H, C), d, sc, ss, bm(border)), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_integral(const void* src, int dt, int W, int H, int C, double* dst, int squared) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::integralImage(wrap<S>(src, W, H, C), squared != 0), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_adaptive_threshold(const void* src, int dt, int W, int H, void* dst, double maxval, int method, int type,
+                           int bs, double c) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::adaptiveThreshold(wrap<S>(src, W, H, 1), maxval, static_cast<AdaptiveMethod>(method),
+                                          static_cast<ThresholdType>(type), bs, c),
+                   dst);
+        });
+        return 0;
+    });
+}
+
+int ref_pyr_down(const void* src, int dt, int W, int H, int C, void* dst) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::pyrDown(wrap<S>(src, W, H, C)), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_pyr_up(const void* src, int dt, int W, int H, int C, void* dst) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::pyrUp(wrap<S>(src, W, H, C)), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_ssim(const void* a, const void* b, int dt, int W, int H, int C, double* result, float* map) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            ImageF m;
+            *result = ipf::ssim(wrap<S>(a, W, H, C), wrap<S>(b, W, H, C), map ? &m : nullptr);
+            if (map) unwrap(m, map);
+        });
+        return 0;
+    });
+}
+
+int ref_corner(const void* src, int dt, int W, int H, float* dst, int bs, int ksize, double k, int min_eig) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            const Image<S> in = wrap<S>(src, W, H, 1);
+            unwrap(min_eig ? ipf::cornerMinEigenVal(in, bs, ksize) : ipf::cornerHarris(in, bs, ksize, k), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_canny(const void* src, int dt, int W, int H, int C, std::uint8_t* dst, double low, double high, int ksize,
+              int l2) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::canny(wrap<S>(src, W, H, C), low, high, ksize, l2 != 0), dst);
         });
         return 0;
     });
