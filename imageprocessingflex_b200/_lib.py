@@ -60,6 +60,7 @@ _SIGNATURES = {
     "ipfc_last_error": (ctypes.c_char_p, []),
     "ipfc_version": (c_int, []),
     "ipfc_check_device": (c_int, [c_void_p]),
+    "ipfc_set_wait_limit_ns": (ctypes.c_ulonglong, [ctypes.c_ulonglong]),
     "ipfc_gaussian_kernel_1d": (c_int, [c_double, c_int, c_void_p, c_int]),
     "ipfc_deriv_kernel": (c_int, [c_int, c_int, c_void_p, c_int]),
     "ipfc_structuring_element": (c_int, [c_int, c_int, c_int, c_void_p]),
@@ -112,6 +113,7 @@ _SIGNATURES = {
     "ipfc_server_poll": (c_int, [c_void_p, ctypes.POINTER(IpfcCompletion), c_int, c_void_p, c_int]),
     "ipfc_server_drain": (c_int, [c_void_p, c_int]),
     "ipfc_server_stats": (c_int, [c_void_p, c_int, c_void_p]),
+    "ipfc_server_fail_allocation": (c_int, [c_void_p, c_longlong]),
     "ipfc_probe_border_index": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
     "ipfc_probe_saturate": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p]),
 }

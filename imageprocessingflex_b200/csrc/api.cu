@@ -130,6 +130,14 @@ unsigned* device_error_word() {
     return w;
 }
 
+// Bound of the device-side pipeline waits of the tensor-core kernels.
+static unsigned long long g_wait_limit_ns = 0;  // 0: the default
+
+unsigned long long device_wait_limit_ns() {
+    const unsigned long long v = __atomic_load_n(&g_wait_limit_ns, __ATOMIC_ACQUIRE);
+    return v ? v : kWaitNsDefault;
+}
+
 // Reads and clears the error word after the stream has drained.
 int take_device_error(cudaStream_t s, const char* fn) {
     unsigned* w = device_error_word();
@@ -283,25 +291,19 @@ bool filter2d_tc_eligible(int sdt, int ddt, int C, int kw, int kh);
 cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spitch, void* dst, long long dpitch, int W,
                                int H, const float* taps, int kw, int kh, int ax, int ay, int border, float delta,
                                float bv, cudaStream_t s);
-bool sep_tc_launch(const void* src, long long spitch, void* dst, long long dpitch, int W, int H, int C,
-                   const double* kx, const double* ky, int K, int border, double delta, double bv, int clamp,
-                   cudaStream_t s, cudaError_t* err);
 bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpitch, int W, int H, int C,
                      const double* kx, const double* ky, int K, int border, double delta, double bv, int clamp,
                      cudaStream_t s, cudaError_t* err);
 
 // Kernel selection for separable filters.  Default: the CUDA-core fast
 // kernel where it is instantiated, else the generic kernels.
-// IPFC_SEP_PATH=generic forces the generic fused/two-pass kernels; =tc
-// selects the tensor-core column-pass kernel (sep_tc.cu) where it is
-// instantiated -- correct, but slower than the fast kernel on B200 so far.
+// IPFC_SEP_PATH=generic forces the generic fused/two-pass kernels; =tcol
+// selects the kernel with the column pass on tcgen05 (sep_tcol.cu) for the
+// uint8 calls it covers.
 static int sep_path_mode() {
     static const int mode = [] {  // read once, thread-safe initialisation
         const char* v = std::getenv("IPFC_SEP_PATH");
-        return (v && std::strcmp(v, "generic") == 0) ? 1
-               : (v && std::strcmp(v, "tc") == 0)    ? 3
-               : (v && std::strcmp(v, "tcol") == 0)  ? 4
-                                                     : 0;
+        return (v && std::strcmp(v, "generic") == 0) ? 1 : (v && std::strcmp(v, "tcol") == 0) ? 4 : 0;
     }();
     return mode;
 }
@@ -393,10 +395,6 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
     if (!make_sep_fast_args(src, dst, in.ptr, in.pitch, out.ptr, out.pitch, kx, kw, ky, kh, ax, ay, border, delta, bv,
                             &f))
         return false;
-    if (sep_path_mode() == 3 && src->dtype == IPFC_U8 && dst->dtype == IPFC_U8 &&
-        sep_tc_launch(in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, kx, ky, kw, border,
-                      delta, bv, f.clamp, s, e))
-        return true;
     if (sep_path_mode() == 4 && src->dtype == IPFC_U8 && dst->dtype == IPFC_U8 &&
         sep_tcol_launch(in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, kx, ky, kw,
                         border, delta, bv, f.clamp, s, e))
@@ -493,6 +491,11 @@ extern "C" {
 const char* ipfc_last_error(void) { return g_last_error.c_str(); }
 
 int ipfc_version(void) { return (1 << 16) | (0 << 8) | 0; }
+
+unsigned long long ipfc_set_wait_limit_ns(unsigned long long ns) {
+    const unsigned long long old = __atomic_exchange_n(&g_wait_limit_ns, ns, __ATOMIC_ACQ_REL);
+    return old ? old : kWaitNsDefault;
+}
 
 int ipfc_check_device(void* stream) {
     int n = 0;

@@ -40,9 +40,11 @@ namespace ipfc {
 int set_error(int code, const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* fn);
 unsigned* device_error_word();
+unsigned long long device_wait_limit_ns();
 cudaError_t ensure_smem_attr(const void* func, int bytes, unsigned* done_mask);
 
-constexpr unsigned kErrTcWait = 0x201u;  // the MMA completion barrier never fired
+constexpr unsigned kErrTcWait = 0x201u;   // a pipeline wait gave up
+constexpr unsigned kErrTcDrain = 0x202u;  // the final MMA drain gave up: tensor memory left allocated
 
 struct F2DTcArgs {
     const void* src;
@@ -59,6 +61,7 @@ struct F2DTcArgs {
     unsigned char bvb;  // that byte
     const uint4* btab;  // B in the shared layout
     unsigned* err;
+    unsigned long long wait_ns;  // bound of a pipeline wait
 };
 
 namespace {
@@ -455,8 +458,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid
             int k = 0;
             for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++k) {
                 const int b = k & 1;
-                if (!mbar_wait(&full[b], (unsigned)(k >> 1) & 1u, a.err, kErrTcWait)) break;
-                if (k >= 2 && !mbar_wait(&tfree[b], (unsigned)((k - 2) >> 1) & 1u, a.err, kErrTcWait)) break;
+                if (!mbar_wait(&full[b], (unsigned)(k >> 1) & 1u, a.err, kErrTcWait, a.wait_ns)) break;
+                if (k >= 2 && !mbar_wait(&tfree[b], (unsigned)((k - 2) >> 1) & 1u, a.err, kErrTcWait, a.wait_ns))
+                    break;
                 tc_fence_after();
                 issue_tile<FSRC>(a, g, sm_base, tbase, b, b);
                 tc_commit(&mma[b]);
@@ -539,7 +543,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid
             const int pb = j & 1;
             int px, py;
             tile_xy(j, px, py);
-            if (mbar_wait(&mma[pb], (unsigned)(j >> 1) & 1u, a.err, kErrTcWait)) {
+            if (mbar_wait(&mma[pb], (unsigned)(j >> 1) & 1u, a.err, kErrTcWait, a.wait_ns)) {
                 tc_fence_after();
                 epilogue_tile<Tout>(a, tbase, pb, px, py, pb ? sc1 : sc0, tid);
                 tc_fence_before();
@@ -561,12 +565,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid
     }
 
     // ---- teardown: every MMA has completed before the columns are freed
+    // (its own bound, not the pipeline's; if even that gives up, the columns
+    // stay allocated rather than freed under a running MMA)
     __syncthreads();
     if (warp == 0) {
-        if (lane == 0) mbar_wait(drained, 0, a.err, kErrTcWait);
-        __syncwarp();
+        bool ok = true;
+        if (lane == 0) ok = mbar_wait(drained, 0, a.err, kErrTcDrain, kDrainNs);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
+        if (ok)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols)
+                         : "memory");
     }
 }
 
@@ -661,6 +670,7 @@ cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spit
                                             (bv >= 0.f && bv <= 255.f && bv == std::floor(bv)))) ? 1 : 0;
         a.bvb = (border == IPFC_BORDER_CONSTANT && a.byte_border) ? (unsigned char)bv : 0;
         a.err = device_error_word();
+        a.wait_ns = device_wait_limit_ns();
         if (sdt == IPFC_F32) e = tc_launch_typed<float, float>(a, g, s);
         else if (ddt == IPFC_U8) e = tc_launch_typed<uint8_t, uint8_t>(a, g, s);
         else if (ddt == IPFC_U16) e = tc_launch_typed<uint8_t, uint16_t>(a, g, s);

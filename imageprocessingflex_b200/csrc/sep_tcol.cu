@@ -42,6 +42,7 @@
 namespace ipfc {
 
 unsigned* device_error_word();
+unsigned long long device_wait_limit_ns();
 cudaError_t ensure_smem_attr(const void* func, int bytes, unsigned* done_mask);
 
 constexpr unsigned kErrTcolWait = 0x301u;   // a pipeline wait gave up
@@ -67,24 +68,18 @@ struct TcolArgs {
 
 namespace {
 
-__device__ __forceinline__ unsigned long long tcol_clock_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
 // Bounded wait on a barrier phase.  The bound is wall time (a.wait_ns on the
 // global timer), not a poll count: try_wait may suspend the thread for a
 // system-dependent time per poll.  Gives up early when another role has set
 // the abort flag; a wait that runs out records kErrTcolWait and sets it.
 __device__ __forceinline__ bool tcol_wait(uint64_t* bar, unsigned parity, const TcolArgs& a, volatile int* abort_flag) {
     if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long t0 = tcol_clock_ns();
+    const unsigned long long t0 = globaltimer_ns();
     for (unsigned i = 1;; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((i & 63u) == 0) {
             if (*abort_flag) return false;
-            if (tcol_clock_ns() - t0 > a.wait_ns) break;
+            if (globaltimer_ns() - t0 > a.wait_ns) break;
         }
     }
     if (a.err) atomicCAS(a.err, 0u, kErrTcolWait);
@@ -392,11 +387,9 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
     if (warp == 0) {
         bool drained = true;
         if (lane == 0) {
-            // every issued MMA completes in microseconds; the bound is 8 waits' worth
-            drained = mbar_try_wait(drain, 0);
-            const unsigned long long t0 = tcol_clock_ns();
-            while (!drained && tcol_clock_ns() - t0 <= 8 * a.wait_ns) drained = mbar_try_wait(drain, 0);
-            if (!drained && a.err) atomicCAS(a.err, 0u, kErrTcolDrain);
+            // every issued MMA completes in microseconds; this bound is its
+            // own, independent of the (possibly shortened) pipeline bound
+            drained = mbar_wait(drain, 0, a.err, kErrTcolDrain, kDrainNs);
         }
         drained = __shfl_sync(0xffffffffu, drained ? 1 : 0, 0) != 0;
         tc_fence_after();
@@ -478,7 +471,7 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
     a.clamp = clamp;
     a.vec_store = (((uintptr_t)dst & 15) == 0 && (dpitch & 15) == 0) ? 1 : 0;
     a.off = (float)(128.0 * sy * sx + delta + 0.5);
-    a.wait_ns = 250ull * 1000 * 1000;  // 250 ms: far above any legitimate stage wait
+    a.wait_ns = device_wait_limit_ns();
     for (int j = 0; j < K; ++j) {
         const double w = std::ldexp(ky[j], ex);
         const __half hi = __double2half(w);

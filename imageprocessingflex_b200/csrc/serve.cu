@@ -114,6 +114,11 @@ struct ipfc_server {
     int used_slots = 0;
     std::thread worker;
 
+    // injected allocation failure: the n-th device-buffer allocation of a
+    // request (1-based, counted by the scheduler) fails (0: none)
+    std::atomic<long long> fail_alloc_nth{0};
+    long long allocs = 0;
+
     // statistics
     std::atomic<long long> st_groups{0}, st_batched{0}, st_batch_launches{0}, st_max_slots{0}, st_failed{0};
     std::atomic<long long> st_max_bytes{0};
@@ -247,11 +252,16 @@ int run_single(const Req& q, cudaStream_t st) {
 void dispatch_group(ipfc_server* s, Group& g, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     // device buffers and input copies
+    auto pool_alloc = [&](void** p, size_t bytes) -> cudaError_t {
+        const long long nth = s->fail_alloc_nth.load();
+        if (nth > 0 && ++s->allocs == nth) return cudaErrorMemoryAllocation;  // injected (host side)
+        return cudaMallocFromPoolAsync(p, bytes, s->pool, st);
+    };
     for (Req& q : g.reqs) {
         const ipfc_request& r = q.r;
         if (r.src.mem == IPFC_MEM_HOST) {
             q.dspitch = row_bytes_of(r.src);
-            e = cudaMallocFromPoolAsync(&q.dsrc, round256((size_t)q.dspitch * r.src.height), s->pool, st);
+            e = pool_alloc(&q.dsrc, round256((size_t)q.dspitch * r.src.height));
             if (e == cudaSuccess)
                 e = cudaMemcpy2DAsync(q.dsrc, (size_t)q.dspitch, r.src.data, (size_t)pitch_of_img(r.src),
                                       (size_t)q.dspitch, (size_t)r.src.height, cudaMemcpyHostToDevice, st);
@@ -261,7 +271,7 @@ void dispatch_group(ipfc_server* s, Group& g, cudaStream_t st) {
         }
         if (e == cudaSuccess && r.dst.mem == IPFC_MEM_HOST) {
             q.ddpitch = row_bytes_of(r.dst);
-            e = cudaMallocFromPoolAsync(&q.ddst, round256((size_t)q.ddpitch * r.dst.height), s->pool, st);
+            e = pool_alloc(&q.ddst, round256((size_t)q.ddpitch * r.dst.height));
         } else if (e == cudaSuccess) {
             q.ddst = r.dst.data;
             q.ddpitch = pitch_of_img(r.dst);
@@ -422,6 +432,12 @@ void scheduler(ipfc_server* s) {
 }  // namespace
 
 extern "C" {
+
+int ipfc_server_fail_allocation(ipfc_server* s, long long nth) {
+    if (!s || nth < 0) return set_error(IPFC_ERR_INVALID, "ipf: server: invalid argument");
+    s->fail_alloc_nth.store(nth);
+    return IPFC_OK;
+}
 
 int ipfc_server_create(ipfc_server** out, const ipfc_server_config* cfg) {
     if (!out) return set_error(IPFC_ERR_INVALID, "ipf: server: null output pointer");

@@ -1,9 +1,9 @@
 // tma.cuh -- mbarrier helpers (bounded waits) for the tcgen05 kernels, sm_100a.
 //
-// Every wait is bounded: try_wait spins at most kSpinLimit times; on expiry
-// the caller's error word gets the given code (first writer wins) and the
-// wait returns false, so a kernel never spins forever and the host can
-// report IPFC_ERR_TIMEOUT.  No multicast form is used anywhere.
+// Every wait is bounded in wall time; on expiry the caller's error word gets
+// the given code (first writer wins) and the wait returns false, so a kernel
+// never spins forever and the host can report IPFC_ERR_TIMEOUT.  No
+// multicast form is used anywhere.
 #pragma once
 
 #include <cuda.h>
@@ -12,9 +12,6 @@
 
 namespace ipfc {
 
-// About 2^24 polls (tens of milliseconds): far above any legitimate wait
-// for a stage of a tensor-core pipeline, short enough to bound a stuck kernel.
-constexpr unsigned kSpinLimit = 1u << 24;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -57,10 +54,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase of the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned* err, unsigned code) {
-    for (unsigned i = 0; i < kSpinLimit; ++i)
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Default bound of a pipeline wait, and the bound of the final drain wait
+// before tensor memory is freed (independent of the pipeline bound, so a
+// shortened pipeline bound never frees memory under a running MMA).
+constexpr unsigned long long kWaitNsDefault = 250ull * 1000 * 1000;
+constexpr unsigned long long kDrainNs = 2000ull * 1000 * 1000;
+
+// Bounded wait for the phase of the given parity to complete.  The bound is
+// wall time on the global timer (try_wait may suspend the thread for a
+// system-dependent time per poll, so a poll count bounds nothing).  On
+// expiry the error word gets `code` (first writer wins) and it returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned* err, unsigned code,
+                                          unsigned long long limit_ns = kWaitNsDefault) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (unsigned i = 1;; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) break;
+    }
     if (err) atomicCAS(err, 0u, code);
     return false;
 }

@@ -116,6 +116,11 @@ class Server:
     def drain(self, timeout_ms: int = -1) -> None:
         _check(self._lib.ipfc_server_drain(self._h, int(timeout_ms)))
 
+    def fail_allocation(self, nth: int) -> None:
+        """Failure injection: the nth device-buffer allocation the server makes
+        for a request fails as out of memory (0 disables)."""
+        _check(self._lib.ipfc_server_fail_allocation(self._h, int(nth)))
+
     def stats(self) -> dict:
         out = {}
         for name, code in STATS.items():

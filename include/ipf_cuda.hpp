@@ -164,5 +164,109 @@ Image<T> dilate(const Image<T>& src, const StructuringElement& se = getStructuri
     return out;
 }
 
+/// morphologyEx (include/ipf/morphology.hpp:140-158).
+template <class T>
+Image<T> morphologyEx(const Image<T>& src, MorphOp op,
+                      const StructuringElement& se = getStructuringElement(MorphShape::Rect, 3), int iterations = 1) {
+    if (se.channels() != 1 || se.empty())
+        throw ipf::Error("ipf: morphology: structuring element must be a non-empty single-channel mask");
+    Image<T> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_morphology_ex(&s, &d, static_cast<int>(op), se.data(), se.width(), se.height(), iterations,
+                                     nullptr));
+    return out;
+}
+
+/// bilateralFilter (include/ipf/filter.hpp:337-387).
+template <class T>
+Image<T> bilateralFilter(const Image<T>& src, int d, double sigmaColor, double sigmaSpace,
+                         BorderMode border = BorderMode::Reflect101) {
+    Image<T> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), o = detail::view(out);
+    detail::check(ipfc_bilateral_filter(&s, &o, d, sigmaColor, sigmaSpace, static_cast<int>(border), nullptr));
+    return out;
+}
+
+/// integralImage (include/ipf/filter.hpp:527-541).
+template <class T>
+ImageD integralImage(const Image<T>& src, bool squared = false) {
+    ImageD out(src.width() + 1, src.height() + 1, src.channels(), 0.0);
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_integral_image(&s, &d, squared ? 1 : 0, nullptr));
+    return out;
+}
+
+/// adaptiveThreshold (include/ipf/filter.hpp:554-567).
+template <class T>
+Image<T> adaptiveThreshold(const Image<T>& src, double maxval, AdaptiveMethod method, ThresholdType type,
+                           int blockSize, double C) {
+    Image<T> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_adaptive_threshold(&s, &d, maxval, static_cast<int>(method), static_cast<int>(type), blockSize,
+                                          C, nullptr));
+    return out;
+}
+
+/// pyrDown (include/ipf/geometry.hpp:504-513).
+template <class T>
+Image<T> pyrDown(const Image<T>& src) {
+    Image<T> out((src.width() + 1) / 2, (src.height() + 1) / 2, src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_pyr_down(&s, &d, nullptr));
+    return out;
+}
+
+/// pyrUp (include/ipf/geometry.hpp:516-525).
+template <class T>
+Image<T> pyrUp(const Image<T>& src) {
+    Image<T> out(src.width() * 2, src.height() * 2, src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_pyr_up(&s, &d, nullptr));
+    return out;
+}
+
+/// ssim (include/ipf/metrics.hpp:51-78).
+template <class T>
+double ssim(const Image<T>& a, const Image<T>& b, ImageF* ssimMap = nullptr) {
+    ipfc_image va = detail::view(a), vb = detail::view(b);
+    ImageF map;
+    ipfc_image vm;
+    if (ssimMap) {
+        map = ImageF(a.width(), a.height(), a.channels());
+        vm = detail::view(map);
+    }
+    double r = 0;
+    detail::check(ipfc_ssim(&va, &vb, &r, ssimMap ? &vm : nullptr, nullptr));
+    if (ssimMap) *ssimMap = std::move(map);
+    return r;
+}
+
+/// cornerHarris (include/ipf/features.hpp:128-136).
+template <class T>
+ImageF cornerHarris(const Image<T>& src, int blockSize = 3, int ksize = 3, double k = 0.04) {
+    ImageF out(src.width(), src.height(), 1);
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_corner_harris(&s, &d, blockSize, ksize, k, nullptr));
+    return out;
+}
+
+/// cornerMinEigenVal (include/ipf/features.hpp:138-146).
+template <class T>
+ImageF cornerMinEigenVal(const Image<T>& src, int blockSize = 3, int ksize = 3) {
+    ImageF out(src.width(), src.height(), 1);
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_corner_min_eigen_val(&s, &d, blockSize, ksize, nullptr));
+    return out;
+}
+
+/// canny (include/ipf/features.hpp:27-88).
+template <class T>
+ImageU8 canny(const Image<T>& src, double lowThreshold, double highThreshold, int ksize = 3, bool l2Gradient = false) {
+    ImageU8 out(src.width(), src.height(), 1);
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_canny(&s, &d, lowThreshold, highThreshold, ksize, l2Gradient ? 1 : 0, nullptr));
+    return out;
+}
+
 }  // namespace cuda
 }  // namespace ipf

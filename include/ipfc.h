@@ -185,6 +185,15 @@ IPFC_API int ipfc_filter2d_split(const ipfc_image* src, ipfc_image* dst, const f
 IPFC_API int ipfc_filter2d_noalloc(const ipfc_image* src, ipfc_image* dst, const float* kernel, int kw, int kh, int ax,
                                    int ay, int border, double delta, double border_value, void* stream);
 
+/* Bound of every device-side wait of the tensor-core kernels (a stage of a
+ * pipeline that never completes), in nanoseconds; 0 restores the default
+ * (250 ms).  A wait that runs out makes the call report IPFC_ERR_TIMEOUT
+ * (ipfc_check_device for device images) and the kernel ends; the final wait
+ * for issued MMAs before tensor memory is freed keeps its own bound.
+ * Returns the previous bound.  No counterpart in the reference (it has no
+ * device waits); tests use it to make a wait run out. */
+IPFC_API unsigned long long ipfc_set_wait_limit_ns(unsigned long long ns);
+
 /* ---- order statistics and morphology -------------------------------------- */
 
 /* medianBlur (filter.hpp:302-332): exact; Constant border is an error. */
@@ -402,6 +411,14 @@ IPFC_API int ipfc_server_submit(ipfc_server* s, const ipfc_request* r, unsigned 
 IPFC_API int ipfc_server_poll(ipfc_server* s, ipfc_completion* out, int max, int* n, int wait_ms);
 IPFC_API int ipfc_server_drain(ipfc_server* s, int timeout_ms); /* < 0: no limit */
 IPFC_API int ipfc_server_stats(const ipfc_server* s, int what, double* value);
+
+/* Failure injection on the host, for tests of the failure path: from now on
+ * the nth device-buffer allocation the server makes for a request (counted
+ * from the server's creation, 1-based; 0 disables) fails as if the
+ * pool were exhausted.  That request completes with IPFC_ERR_NOMEM and runs
+ * no kernel; every other request completes normally.  No counterpart in the
+ * reference (it has no request server). */
+IPFC_API int ipfc_server_fail_allocation(ipfc_server* s, long long nth);
 
 /* ---- device probes of the scalar rules --------------------------------- */
 

@@ -8,7 +8,10 @@
 // integer-tap (Sobel) filters; within 1 LSB for FP32-accumulated uint8
 // outputs (mismatch rate printed); 1e-5 relative for float outputs.  It also
 // checks that argument errors throw ipf::Error with the reference's text.
+#include <ipf/features.hpp>
 #include <ipf/filter.hpp>
+#include <ipf/geometry.hpp>
+#include <ipf/metrics.hpp>
 #include <ipf/morphology.hpp>
 #include <ipf_cuda.hpp>
 
@@ -117,6 +120,41 @@ int main() {
         compare(buf, cuda::dilate(rgb, se), dilate(rgb, se), 0, 0);
     }
     compare("erode default 3x3 rect gray", cuda::erode(gray), erode(gray), 0, 0);
+    // int32 / double images and TOut = double: FP64 in the reference's order, exact
+    const ImageD grayd = seeded<double>(331, 217, 1, 11);
+    const ImageI32 grayi = seeded<std::int32_t>(331, 217, 3, 12);
+    compare("gaussianBlur ImageD sigma 1.5", cuda::gaussianBlur(grayd, 1.5), gaussianBlur(grayd, 1.5), 0, 0);
+    compare("gaussianBlur<double> of uint8 RGB", cuda::gaussianBlur<double>(rgb, 2.0), gaussianBlur<double>(rgb, 2.0),
+            0, 0);
+    compare("filter2D ImageI32", cuda::filter2D(grayi, makeKernel(3, 3, {1, -2, 1, 2, 0, -2, 1, 2, 1})),
+            filter2D(grayi, makeKernel(3, 3, {1, -2, 1, 2, 0, -2, 1, 2, 1})), 0, 0);
+    compare("medianBlur 5 ImageD", cuda::medianBlur(grayd, 5), medianBlur(grayd, 5), 0, 0);
+    // the reference's other filters and its callers of the filters
+    compare("morphologyEx Gradient 5x5 ellipse RGB",
+            cuda::morphologyEx(rgb, MorphOp::Gradient, getStructuringElement(MorphShape::Ellipse, 5)),
+            morphologyEx(rgb, MorphOp::Gradient, getStructuringElement(MorphShape::Ellipse, 5)), 0, 0);
+    compare("morphologyEx TopHat 15x15 rect gray",
+            cuda::morphologyEx(gray, MorphOp::TopHat, getStructuringElement(MorphShape::Rect, 15)),
+            morphologyEx(gray, MorphOp::TopHat, getStructuringElement(MorphShape::Rect, 15)), 0, 0);
+    compare("bilateralFilter d 9 RGB", cuda::bilateralFilter(rgb, 9, 50.0, 3.0), bilateralFilter(rgb, 9, 50.0, 3.0), 0,
+            0);
+    compare("integralImage RGB", cuda::integralImage(rgb), integralImage(rgb), 0, 0);
+    compare("adaptiveThreshold Gaussian 11", cuda::adaptiveThreshold(gray, 255.0, AdaptiveMethod::Gaussian,
+                                                                   ThresholdType::Binary, 11, 2.0),
+            adaptiveThreshold(gray, 255.0, AdaptiveMethod::Gaussian, ThresholdType::Binary, 11, 2.0), 0, 0);
+    compare("pyrDown RGB", cuda::pyrDown(rgb), pyrDown(rgb), 0, 0);
+    compare("pyrUp gray", cuda::pyrUp(gray), pyrUp(gray), 0, 0);
+    compare("canny RGB 50 150", cuda::canny(rgb, 50.0, 150.0), canny(rgb, 50.0, 150.0), 0, 0);
+    compare("cornerHarris gray", cuda::cornerHarris(gray), cornerHarris(gray), 0, 1e-5);
+    {
+        ImageF mg, mr;
+        const ImageU8 other = seeded<std::uint8_t>(1920, 1080, 3, 2);
+        const double g = cuda::ssim(rgb, other, &mg), r = ssim(rgb, other, &mr);
+        compare("ssim map RGB", mg, mr, 0, 0);
+        const bool ok = std::fabs(g - r) <= 1e-12 * std::fmax(1.0, std::fabs(r));
+        std::printf("%s %-52s %.17g vs %.17g\n", ok ? "ok  " : "FAIL", "ssim mean RGB", g, r);
+        g_fail += !ok;
+    }
     expect_error("medianBlur even ksize throws", "ipf: medianBlur: ksize must be odd and positive",
                  [&] { (void)cuda::medianBlur(gray, 4); });
     expect_error("medianBlur Constant throws", "ipf: medianBlur: Constant border is not supported",
