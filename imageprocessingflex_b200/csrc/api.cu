@@ -236,6 +236,22 @@ int check_pair(const ipfc_image* src, const ipfc_image* dst, const char* fn, boo
     return IPFC_OK;
 }
 
+// check_pair for a destination whose shape differs from the source's by the
+// function's definition (pyramids, the integral image, single-channel edge
+// maps): the caller has checked that shape; the destination's own pitch is
+// checked against its own row, the rest as check_pair does.
+int check_pair_resized(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type) {
+    if (!src || !dst) return set_error(IPFC_ERR_INVALID, "ipf: %s: null image", fn);
+    if (dtype_supported(dst->dtype) && dst->pitch != 0 && dst->pitch < row_bytes(dst))
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: pitch smaller than a row", fn);
+    ipfc_image same = *dst;
+    same.width = src->width;
+    same.height = src->height;
+    same.channels = src->channels;
+    same.pitch = 0;
+    return check_pair(src, &same, fn, same_type);
+}
+
 // ---------------------------------------------------------------------------
 // Tap generators (FP64, the reference's expressions and order)
 // ---------------------------------------------------------------------------
@@ -289,7 +305,7 @@ int deriv_taps(int order, int ksize, std::vector<double>& k) {
 
 bool filter2d_tc_eligible(int sdt, int ddt, int C, int kw, int kh);
 cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spitch, void* dst, long long dpitch, int W,
-                               int H, const float* taps, int kw, int kh, int ax, int ay, int border, float delta,
+                               int H, int C, const float* taps, int kw, int kh, int ax, int ay, int border, float delta,
                                float bv, cudaStream_t s);
 bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpitch, int W, int H, int C,
                      const double* kx, const double* ky, int K, int border, double delta, double bv, int clamp,
@@ -662,8 +678,8 @@ namespace ipfc {
 // split-precision tensor-core kernel (filter2d_tc.cu).
 enum F2DForm { kF2DAuto = 0, kF2DFp32 = 1, kF2DSplit = 2 };
 
-// Automatic choice: the tensor-core form for single-channel uint8 sources
-// and kernels of 15 x 15 taps and more (many times faster than the FP32 form,
+// Automatic choice: the tensor-core form for uint8 sources (1, 3 or 4
+// channels) and kernels of 15 x 15 taps and more (many times faster than the FP32 form,
 // with uint8 pixels exact and an error against the FP64 reference on a par
 // with it), the FP32 CUDA-core form otherwise.  IPFC_F2D_PATH=split selects
 // the tensor-core form wherever it applies, =fp32 pins the CUDA-core form.
@@ -692,8 +708,8 @@ static int run_filter2d(const ipfc_image* src, ipfc_image* dst, const float* ker
     if (rc) return rc;
     if (form == kF2DSplit && !filter2d_tc_eligible(src->dtype, dst->dtype, src->channels, kw, kh))
         return set_error(IPFC_ERR_UNSUPPORTED,
-                         "ipf: %s: the tensor-core form takes single-channel uint8 (to uint8, uint16, int16, float) "
-                         "or float (to float) images and kernels up to %dx%d",
+                         "ipf: %s: the tensor-core form takes uint8 (to uint8, uint16, int16, float; 1, 3 or 4 "
+                         "channels) or single-channel float (to float) images and kernels up to %dx%d",
                          fn, kTcMaxKw, kTcMaxKh);
     if (form == kF2DAuto) form = f2d_auto_form(src, dst, kw, kh);
     cudaStream_t s = (cudaStream_t)stream;
@@ -731,7 +747,7 @@ static int run_filter2d(const ipfc_image* src, ipfc_image* dst, const float* ker
     a.dpitch = out.pitch;
     if (form == kF2DSplit) {
         cudaError_t e = filter2d_tc_launch(src->dtype, dst->dtype, in.ptr, in.pitch, out.ptr, out.pitch, a.W, a.H,
-                                           kernel, kw, kh, ax, ay, border, (float)delta, (float)border_value, s);
+                                           a.C, kernel, kw, kh, ax, ay, border, (float)delta, (float)border_value, s);
         rc = finish(dst, &in, &out, s, fn);
         if (e != cudaSuccess) return cuda_status(e, fn);
         return rc;

@@ -24,6 +24,7 @@ int take_device_error(cudaStream_t s, const char* fn);
 // Checks a source/destination pair: IPFC_OK, an error, or -1 for an empty
 // image (nothing to do).
 int check_pair(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type);
+int check_pair_resized(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type);
 
 // A device view of an image: the caller's memory, or a staged copy.
 struct DevView {

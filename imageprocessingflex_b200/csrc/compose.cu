@@ -356,11 +356,7 @@ extern "C" int ipfc_integral_image(const ipfc_image* src, ipfc_image* dst, int s
         return set_error(IPFC_ERR_INVALID, "ipf: %s: the integral image is double (ImageD)", fn);
     if (dst->width != src->width + 1 || dst->height != src->height + 1 || dst->channels != src->channels)
         return set_error(IPFC_ERR_INVALID, "ipf: %s: destination must be (W+1) x (H+1) with the source's channels", fn);
-    // the shape check of check_pair compares equal sizes: check the source alone
-    ipfc_image same = *dst;
-    same.width = src->width;
-    same.height = src->height;
-    int rc = check_pair(src, &same, fn, false);
+    int rc = check_pair_resized(src, dst, fn, false);
     if (rc == -1) {
         // empty source: I is a single zero row / column
         if (dst->width <= 0 || dst->height <= 0) return IPFC_OK;
@@ -514,10 +510,7 @@ extern "C" int ipfc_pyr_down(const ipfc_image* src, ipfc_image* dst, void* strea
     const int W2 = (src->width + 1) / 2, H2 = (src->height + 1) / 2;
     if (dst->width != W2 || dst->height != H2 || dst->channels != src->channels || dst->dtype != src->dtype)
         return set_error(IPFC_ERR_INVALID, "ipf: %s: destination must be ((W+1)/2) x ((H+1)/2), same type", fn);
-    ipfc_image same = *dst;
-    same.width = src->width;
-    same.height = src->height;
-    int rc = check_pair(src, &same, fn, true);
+    int rc = check_pair_resized(src, dst, fn, true);
     if (rc == -1) return IPFC_OK;
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
@@ -558,10 +551,7 @@ extern "C" int ipfc_pyr_up(const ipfc_image* src, ipfc_image* dst, void* stream)
     if (dst->width != 2 * src->width || dst->height != 2 * src->height || dst->channels != src->channels ||
         dst->dtype != src->dtype)
         return set_error(IPFC_ERR_INVALID, "ipf: %s: destination must be 2W x 2H, same type", fn);
-    ipfc_image same = *dst;
-    same.width = src->width;
-    same.height = src->height;
-    int rc = check_pair(src, &same, fn, true);
+    int rc = check_pair_resized(src, dst, fn, true);
     if (rc == -1) return IPFC_OK;
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;

@@ -507,9 +507,7 @@ extern "C" int ipfc_canny(const ipfc_image* src, ipfc_image* dst, double low_thr
     if (!src || !dst) return set_error(IPFC_ERR_INVALID, "ipf: %s: null image", fn);
     if (dst->dtype != IPFC_U8 || dst->channels != 1 || dst->width != src->width || dst->height != src->height)
         return set_error(IPFC_ERR_INVALID, "ipf: %s: the edge map is uint8, single channel, the source's size", fn);
-    ipfc_image same = *dst;
-    same.channels = src->channels;
-    int rc = check_pair(src, &same, fn, false);
+    int rc = check_pair_resized(src, dst, fn, false);
     if (rc == -1) return IPFC_OK;
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;

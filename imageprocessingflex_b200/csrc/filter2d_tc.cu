@@ -52,6 +52,7 @@ struct F2DTcArgs {
     void* dst;
     long long dpitch;
     int W, H, border;
+    int C, rowlen;  // channels; samples per row (W * C)
     float delta, bv;
     int kw, kh, ax, ay;
     float tap_unscale;  // 2^-s
@@ -82,10 +83,10 @@ constexpr int kOddCol = 32;
 // (gy0, gx0), borders resolved (-1: the Constant border value).
 template <typename Tin>
 __device__ __forceinline__ void load_item(const F2DTcArgs& a, int gy0, int gx0, float (&v)[8][4]) {
-    const bool cols_in = gx0 >= 0 && gx0 + 4 <= a.W;
+    const bool cols_in = gx0 >= 0 && gx0 + 4 <= a.rowlen;
     int cx[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) cx[c] = cols_in ? gx0 + c : border_index(gx0 + c, a.W, a.border);
+    for (int c = 0; c < 4; ++c) cx[c] = cols_in ? gx0 + c : border_sample(gx0 + c, a.W, a.C, a.border);
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const int sy = border_index(gy0 + j, a.H, a.border);
@@ -126,15 +127,17 @@ struct TileScale {
     float offset;   // centre * sum(taps) + delta
 };
 
-constexpr int kTcItemsPerThread = 2;  // staging items per worker (XR/4 x KR/8 <= 42 x 12 <= 512)
+// staging items per worker: XR/4 x KR/8 items per tile, at most 42 x 12 for
+// one channel and 64 x 12 for up to 4 channels (uint8 only)
+__host__ __device__ constexpr int tc_items_per_thread(bool float_src) { return float_src ? 2 : 3; }
 
 // uint8 source, prefetch form: 8 rows x 4 pixels at (gy0, gx0) as one word
 // (4 bytes) per row, borders resolved, Constant as the border byte.
 __device__ __forceinline__ void load_item_raw(const F2DTcArgs& a, int gy0, int gx0, unsigned (&w)[8]) {
-    const bool cols_in = gx0 >= 0 && gx0 + 4 <= a.W;
+    const bool cols_in = gx0 >= 0 && gx0 + 4 <= a.rowlen;
     int cx[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) cx[c] = cols_in ? gx0 + c : border_index(gx0 + c, a.W, a.border);
+    for (int c = 0; c < 4; ++c) cx[c] = cols_in ? gx0 + c : border_sample(gx0 + c, a.W, a.C, a.border);
     const unsigned cfill = 0x01010101u * a.bvb;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -355,7 +358,7 @@ __device__ __forceinline__ void epilogue_tile(const F2DTcArgs& a, uint32_t tbase
 #pragma unroll
             for (int n = 0; n < 16; ++n) u[n] = z[n] = 0.f;
         }
-        if (x < a.W) {
+        if (x < a.rowlen) {
 #pragma unroll
             for (int n = 0; n < 16; ++n) {
                 const int y = ty0 + kTcN * gi + n;
@@ -387,7 +390,7 @@ __device__ __forceinline__ void issue_tile(const F2DTcArgs& a, const TcGeom& g, 
         uint32_t first[2] = {0u, 0u};  // accumulate flags of the even and odd accumulators
         for (int i = 0; i < a.kw; ++i) {
             const uint32_t dm = d0 + (uint32_t)((i & 1) * kOddCol), dc = dm + (uint32_t)kCorrCol;
-            const uint32_t ash16 = (uint32_t)(i + g.axa - a.ax);  // 16-byte rows
+            const uint32_t ash16 = (uint32_t)(i * g.C + g.axa - g.axs);  // 16-byte rows
             const uint32_t bi16 = (uint32_t)(i * g.bytesBi) >> 4;
             uint32_t acc = first[i & 1];
 #pragma unroll 4
@@ -415,7 +418,7 @@ template <typename Tin, typename Tout>
 __global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid_constant__ F2DTcArgs a) {
     constexpr bool FSRC = sizeof(Tin) == 4;
     extern __shared__ __align__(1024) unsigned char sm[];
-    const TcGeom g(a.kw, a.kh, a.ax, a.ay, FSRC);
+    const TcGeom g(a.kw, a.kh, a.ax, a.ay, FSRC, a.C);
     uint64_t* full = reinterpret_cast<uint64_t*>(sm + g.offBar);   // [2]
     uint64_t* mma = full + 2;                                        // [2]
     uint64_t* tfree = full + 4;                                      // [2]
@@ -485,6 +488,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) filter2d_tc_kernel(const __grid
             tx0 = (t % a.tiles_x) * kTcM;
             ty0 = (t / a.tiles_x) * kTcRows;
         };
+        constexpr int kTcItemsPerThread = tc_items_per_thread(FSRC);
         unsigned raw[kTcItemsPerThread][8];
         float fv[FSRC ? kTcItemsPerThread : 1][8][4];
         auto issue_loads = [&](int j) {
@@ -629,15 +633,24 @@ void tc_build_b(const TcGeom& g, const float* taps, std::vector<__half>& out, fl
             }
 }
 
+// Single-channel images of the supported types, and uint8 images of 3 or 4
+// interleaved channels, while the staged tile fits shared memory and the
+// staging items fit the workers.
 bool filter2d_tc_eligible(int sdt, int ddt, int C, int kw, int kh) {
-    return C == 1 && tc_supported(sdt, ddt) && kw >= 1 && kh >= 1 && kw <= kTcMaxKw && kh <= kTcMaxKh;
+    if (!(tc_supported(sdt, ddt) && kw >= 1 && kh >= 1 && kw <= kTcMaxKw && kh <= kTcMaxKh)) return false;
+    if (!(C == 1 || ((C == 3 || C == 4) && sdt == IPFC_U8))) return false;
+    const TcGeom g(kw, kh, kw / 2, kh / 2, sdt == IPFC_F32, C);
+    const int items = (g.XR / 4) * (g.KR / 8);
+    return g.smem <= 227 * 1024 && items <= tc_items_per_thread(sdt == IPFC_F32) * kTcWorkers;
 }
 
 // Launches the tensor-core form; taps are the dense kw x kh kernel (host).
 cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spitch, void* dst, long long dpitch, int W,
-                               int H, const float* taps, int kw, int kh, int ax, int ay, int border, float delta,
+                               int H, int C, const float* taps, int kw, int kh, int ax, int ay, int border, float delta,
                                float bv, cudaStream_t s) {
-    const TcGeom g(kw, kh, ax, ay, sdt == IPFC_F32);
+    const TcGeom g(kw, kh, ax, ay, sdt == IPFC_F32, C);
+    if (g.smem > 227 * 1024 || (g.XR / 4) * (g.KR / 8) > tc_items_per_thread(sdt == IPFC_F32) * kTcWorkers)
+        return cudaErrorInvalidConfiguration;
     std::vector<__half> bt;
     F2DTcArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -656,6 +669,8 @@ cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spit
         a.dpitch = dpitch;
         a.W = W;
         a.H = H;
+        a.C = C;
+        a.rowlen = W * C;
         a.border = border;
         a.delta = delta;
         a.bv = bv;
@@ -663,7 +678,7 @@ cudaError_t filter2d_tc_launch(int sdt, int ddt, const void* src, long long spit
         a.kh = kh;
         a.ax = ax;
         a.ay = ay;
-        a.tiles_x = (W + kTcM - 1) / kTcM;
+        a.tiles_x = (W * C + kTcM - 1) / kTcM;
         a.ntiles = a.tiles_x * ((H + kTcRows - 1) / kTcRows);
         a.btab = dbt;
         a.byte_border = (sdt == IPFC_U8 && (border != IPFC_BORDER_CONSTANT ||

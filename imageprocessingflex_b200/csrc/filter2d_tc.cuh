@@ -15,6 +15,9 @@
 // where T[x'][r] = P[ty0 - ay + r][tx0 - axa + x'] is the source tile stored
 // transposed (x' major, source rows r contiguous) and axa = ax rounded up to
 // a multiple of 4 (so staged pixel quads start 4-aligned in the image).
+// Images of C > 1 interleaved channels are the same correlation over the row
+// of W*C samples with the horizontal taps C samples apart: x counts samples,
+// the anchor is ax*C samples and tap column i shifts A by i*C rows.
 // Both operands are K-major without swizzle: 8 x 16-byte core matrices,
 // rows 16 bytes apart, so shifting A by one pixel (the tap offset i) is a
 // 16-byte move of the descriptor's start address -- one staged tile serves
@@ -48,7 +51,9 @@ constexpr int kTcMaxKh = 33;
 
 struct TcGeom {
     int kw, kh, ax, ay;
-    int axa;     // ax rounded up to a multiple of 4
+    int C;       // channels: the row is W*C interleaved samples, tap column i sits i*C samples away
+    int axs;     // the anchor in samples (ax * C)
+    int axa;     // axs rounded up to a multiple of 4
     int Kt;      // K of one group's window (>= kh + 15, multiple of 16)
     int XR;      // staged pixels per tile row (multiple of 8)
     int KR;      // staged source rows (multiple of 8)
@@ -61,14 +66,16 @@ struct TcGeom {
     int offBar;
     int smem;
 
-    __host__ __device__ TcGeom(int kw_, int kh_, int ax_, int ay_, bool float_src) {
+    __host__ __device__ TcGeom(int kw_, int kh_, int ax_, int ay_, bool float_src, int C_ = 1) {
         kw = kw_;
         kh = kh_;
         ax = ax_;
         ay = ay_;
-        axa = (ax + 3) / 4 * 4;
+        C = C_;
+        axs = ax * C;
+        axa = (axs + 3) / 4 * 4;
         Kt = (kh + 15 + 15) / 16 * 16;
-        XR = (kTcM + kw - 1 + (axa - ax) + 7) / 8 * 8;
+        XR = (kTcM + (kw - 1) * C + (axa - axs) + 7) / 8 * 8;
         KR = 16 * (kTcGroups - 1) + Kt;
         lboA = XR * 16;
         bytesA = (KR / 8) * lboA;

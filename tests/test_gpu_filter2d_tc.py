@@ -93,10 +93,69 @@ def test_split_device_tensors_match_host(gpu):
     np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize("c", [3, 4])
+def test_split_u8_interleaved_channels_vs_oracle(gpu, orc, c):
+    """3- and 4-channel uint8 images: the row of W*C samples with the taps C
+    samples apart; the same 1-LSB bar, every border."""
+    for w, h in ((1, 1), (7, 3), (130, 65), (333, 129)):
+        img = oracle.random_image(w, h, c, np.uint8, 7 * w + h + c)
+        for kw, kh, anchor in ((15, 15, (-1, -1)), (31, 31, (-1, -1)), (16, 9, (3, 8)), (5, 33, (4, 0))):
+            k = _taps(kh, kw, kw * 100 + kh + c)
+            for b in oracle.BORDERS:
+                got = ipf.filter2D(img, k, ipf.BorderMode(b), 0.5, anchor, 7.0, form="split")
+                want = orc.filter2d(img, k, b, 0.5, anchor, 7.0)
+                d = np.abs(got.astype(int) - want.astype(int))
+                assert d.max(initial=0) <= 1, (w, h, kw, kh, b, d.max())
+        got = ipf.filter2D(img, k, ipf.BorderMode.Reflect101, 0.0, (-1, -1), 0.0, dtype=np.float32, form="split")
+        want = orc.filter2d(img, k, oracle.REFLECT101, 0.0, (-1, -1), 0.0, np.float32)
+        G.compare(got, want, G.tolerance("filter2d", {"border_value": 0.0, "delta": 0.0}, {"src": img, "kernel": k},
+                                         want))
+
+
 def test_split_rejects_what_it_does_not_cover(gpu):
-    img3 = oracle.random_image(40, 30, 3, np.uint8, 1)
+    img3 = oracle.random_image(40, 30, 3, np.float32, 1)
     with pytest.raises(ipf.Error, match="tensor-core form"):
         ipf.filter2D(img3, _taps(15, 15, 1), form="split")
     img = oracle.random_image(40, 30, 1, np.uint8, 1)
     with pytest.raises(ipf.Error, match="tensor-core form"):
         ipf.filter2D(img, _taps(15, 40, 1), form="split")
+
+
+def test_register_tiled_fp32_form_equals_the_general_one(gpu, tmp_path):
+    """The register-tiled FP32 kernel (1 and 3 channels, 9..32 taps per row)
+    repeats the general FP32 kernel's accumulation sequence, so their
+    outputs are bit-identical; the general one is forced in a child process
+    with IPFC_F2D_TILED=0."""
+    import os
+    import subprocess
+    import sys
+
+    code = r'''
+import sys, numpy as np, imageprocessingflex_b200 as ipf, oracle
+out = {}
+for c in (1, 3):
+    for dt in (np.uint8, np.float32):
+        img = oracle.random_image(517, 203, c, dt, 7 + c)
+        for kw, kh in ((9, 9), (15, 15), (16, 3), (31, 31), (32, 33), (13, 21)):
+            if c == 3 and kw > 16:
+                continue
+            rng = np.random.default_rng(kw * 100 + kh)
+            k = rng.normal(size=(kh, kw)).astype(np.float32)
+            k /= k.sum()
+            for b in range(5):
+                for od in (None, np.float32):
+                    key = f"{c}_{np.dtype(dt).name}_{kw}x{kh}_{b}_{od is None}"
+                    out[key] = ipf.filter2D(img, k, ipf.BorderMode(b), 0.5, (-1, -1), 7.0, dtype=od, form="fp32")
+np.savez(sys.argv[1], **out)
+'''
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for tiled in ("1", "0"):
+        f = str(tmp_path / f"out_{tiled}.npz")
+        env = dict(os.environ, IPFC_F2D_TILED=tiled, PYTHONPATH=root)
+        r = subprocess.run([sys.executable, "-c", code, f], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-3000:]
+        res[tiled] = np.load(f)
+    assert set(res["1"].files) == set(res["0"].files) and len(res["1"].files) > 50
+    for key in res["1"].files:
+        np.testing.assert_array_equal(res["1"][key], res["0"][key], err_msg=key)
