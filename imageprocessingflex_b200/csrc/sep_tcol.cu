@@ -10,10 +10,10 @@
 //    lane 0 issues, per step, KR/16 K steps x (A_hi, A_lo) MMAs into the
 //    step's buffer and commits them to the B-empty and T-full barriers;
 //  * warps 1-4 (producers): per step, load the band's KR source rows of the
-//    slab (16-byte loads; rows and samples outside the image resolved by the
-//    border mode, Constant as the border value), convert uint8 - 128 to FP16
-//    exactly (byte permutes into 0x64xx, minus 1152) and store them into one
-//    of two B buffers;
+//    slab (16-byte loads; at the image's edges 16 independent byte loads of
+//    border-resolved samples, Constant as the border byte), convert
+//    uint8 - 128 to FP16 exactly (byte permutes into 0x64xx, minus 1152) and
+//    store them into one of two B buffers;
 //  * warps 5-12 (row pass): warp w reads tensor-memory lanes 32 (w mod 4) ..
 //    +31 -- one output row per thread -- and half the slab's columns, plus
 //    C*(K/2) columns either side from the neighbouring slab buffers; runs the
@@ -55,32 +55,31 @@ struct TcolArgs {
     long long dpitch;
     int W, H, rowlen;
     int border;
-    unsigned short bvh;  // FP16 bits of (Constant border value - 128)
+    unsigned bvb;        // the Constant border value (a byte)
     int nb, ns, units;   // bands, slabs per band, nb * ns
     int clamp;           // outputs may leave [0, 255]
     int vec_store;       // destination base and pitch are 16-byte aligned
     float off;           // 128 * sum(ky) * sum(kx) + delta + 0.5
     unsigned long long wait_ns;   // a pipeline wait gives up after this long
     unsigned short ahi[kTcolMaxK + 1], alo[kTcolMaxK + 1];  // FP16 bits of ky * 2^e (hi, lo)
-    float kx[kTcolMaxK + 1];                                 // kx * 2^-e
+    unsigned long long kx2[kTcolMaxK + 1];                   // kx * 2^-e in both FP32 lanes
     unsigned* err;
 };
 
 namespace {
 
-// Bounded wait on a barrier phase.  The bound is wall time (a.wait_ns on the
-// global timer), not a poll count: try_wait may suspend the thread for a
-// system-dependent time per poll.  Gives up early when another role has set
-// the abort flag; a wait that runs out records kErrTcolWait and sets it.
+// Bounded wait on a barrier phase.  The bound is wall time (a.wait_ns on
+// the global timer), not a poll count: each poll may suspend the thread.
+// Gives up early when another role has set the abort flag; a wait that runs
+// out records kErrTcolWait and sets it.
 __device__ __forceinline__ bool tcol_wait(uint64_t* bar, unsigned parity, const TcolArgs& a, volatile int* abort_flag) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
-    for (unsigned i = 1;; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 63u) == 0) {
-            if (*abort_flag) return false;
-            if (globaltimer_ns() - t0 > a.wait_ns) break;
-        }
+    for (;;) {
+        // sleeps (up to 50 us per poll) rather than spinning
+        if (mbar_try_wait_sleep(bar, parity, 50000u)) return true;
+        if (*abort_flag) return false;
+        if (globaltimer_ns() - t0 > a.wait_ns) break;
     }
     if (a.err) atomicCAS(a.err, 0u, kErrTcolWait);
     *abort_flag = 1;
@@ -117,11 +116,98 @@ __device__ __forceinline__ void tcol_cvt_word(unsigned w, unsigned& h01, unsigne
     h23 = h2_bits(__hsub2(*reinterpret_cast<const __half2*>(&u23), k1152));
 }
 
-// FP16 bits of one border-resolved sample (slow path: edges of the image).
-__device__ __forceinline__ unsigned short tcol_sample_h(const TcolArgs& a, const unsigned char* srow, int g, int C) {
-    const int sx = srow ? border_sample(g, a.W, C, a.border) : -1;
-    if (sx < 0) return a.bvh;
-    return __half_as_ushort(__float2half_rn((float)srow[sx] - 128.f));
+// 16 samples of source row srow (a row of the image) at the
+// border-resolved sample indices sx (-1: Constant), packed
+// as bytes, Constant as the border byte.  The 16 loads are unconditional (a
+// Constant sample reads the row's first byte and is replaced afterwards), so
+// that no branch separates them.
+__device__ __forceinline__ uint4 tcol_gather16(const TcolArgs& a, const unsigned char* srow, const int (&sx)[16]) {
+    unsigned b[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) b[e] = __ldg(srow + (sx[e] >= 0 ? sx[e] : 0));
+    unsigned w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int e = 0; e < 16; ++e) w[e >> 2] |= (sx[e] >= 0 ? b[e] : a.bvb) << (8 * (e & 3));
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Two FP32 lanes in one 64-bit register pair (low: first).
+__device__ __forceinline__ uint64_t tcol_pack2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void tcol_unpack2(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+// d = a * b + c on both lanes, each rounded to nearest: the same result as
+// two fmaf.
+__device__ __forceinline__ uint64_t tcol_fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// Horizontal taps of one 16-output chunk of a row, from the chunk's window
+// v (group 0 = 16*GH columns left of the chunk), rounded and packed as 16
+// bytes.  Output o = off + sum_i kx[i] v[o + C (i - K/2)], two outputs per
+// packed FMA:
+//  * taps whose offset C (i - K/2) is even read aligned register pairs for
+//    the output pairs (2k, 2k+1) -- accumulators E[k], started at off;
+//  * taps with odd offsets (odd C only) read aligned pairs for the output
+//    pairs (2k-1, 2k) -- accumulators O[k], started at 0 -- and
+//    acc(o) = E + O at the end.
+// The FP32 sum order differs from one FMA chain only by that final add.
+template <int K, int C, int GH>
+__device__ __forceinline__ void tcol_row_chunk(const TcolArgs& a, const float (&v)[1 + 2 * GH][16],
+                                               unsigned (&words)[4]) {
+    constexpr int H2 = K / 2;
+    constexpr bool kOdd = (C & 1) != 0;
+    static_assert(!kOdd || 16 * GH >= C * H2 + 1, "odd-offset pairs stay inside the window");
+    auto pair = [&](int c) -> uint64_t { return tcol_pack2(v[c >> 4][c & 15], v[(c + 1) >> 4][(c + 1) & 15]); };
+    const uint64_t off2 = tcol_pack2(a.off, a.off);
+    uint64_t E[8], O[kOdd ? 9 : 1];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) E[k] = off2;
+#pragma unroll
+    for (int k = 0; k < (kOdd ? 9 : 1); ++k) O[k] = 0ull;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        const int d = C * (i - H2) + 16 * GH;
+        const uint64_t kk = a.kx2[i];
+        if (((C * (i - H2)) & 1) == 0) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) E[k] = tcol_fma2(kk, pair(2 * k + d), E[k]);
+        } else if constexpr (kOdd) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) O[k] = tcol_fma2(kk, pair(2 * k - 1 + d), O[k]);
+        }
+    }
+    float acc[16];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) tcol_unpack2(E[k], acc[2 * k], acc[2 * k + 1]);
+    if constexpr (kOdd) {
+        float ol[9], oh[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) tcol_unpack2(O[k], ol[k], oh[k]);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            acc[2 * k] += oh[k];
+            acc[2 * k + 1] += ol[k + 1];
+        }
+    }
+#pragma unroll
+    for (int t4 = 0; t4 < 4; ++t4) {
+        unsigned wd = 0;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            float x = acc[4 * t4 + t];
+            if (a.clamp) x = fminf(fmaxf(x, 0.f), 255.f);
+            const float r = __fadd_rd(x, 8388608.0f);
+            wd = __byte_perm(wd, __float_as_uint(r), byte_insert_sel(t));
+        }
+        words[t4] = wd;
+    }
 }
 
 }  // namespace
@@ -135,7 +221,7 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
     constexpr int GH = tcol_halo_groups(K, C);  // halo groups of 16 columns either side
     constexpr int R = C * (K / 2);
     static_assert(GH <= 2, "row-pass window: at most 32 columns of halo");
-    constexpr int NG = 4 + 2 * GH;  // column groups one row-pass thread reads per step
+    constexpr int NG = 1 + 2 * GH;  // column groups one row-pass chunk reads
 
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + tcol_off_bar(K));
     uint64_t* bfull = bars;        // [2] producers -> MMA
@@ -164,11 +250,16 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
         fence_barrier_init();
     }
     if (warp == 0) tmem_alloc(tslot, kTcolTmemCols);
+    // the taps into shared memory first: the A build below indexes them by
+    // lane, which the parameter bank would serve one address at a time
+    unsigned short* taps = reinterpret_cast<unsigned short*>(bars + 16);  // [2][32]
+    if (tid < 2 * 32) taps[tid] = (tid & 32) ? a.alo[tid & 31] : a.ahi[tid & 31];
+    __syncthreads();
     // A: one 16-byte core-matrix row (fixed m, 8 consecutive k) per item
     for (int it = tid; it < 2 * kTcolM * KG; it += kTcolThreads) {
         const int hl = it / (kTcolM * KG), rest = it % (kTcolM * KG);
         const int m = rest % kTcolM, kg = rest / kTcolM;
-        const unsigned short* tap = hl ? a.alo : a.ahi;
+        const unsigned short* tap = taps + 32 * hl;
         unsigned w[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -225,73 +316,85 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
         __syncwarp();
     } else if (warp <= kTcolProdWarps) {
         // ------------------------------------------------------------ producers
+        // Each lane loads and converts the same items of every step -- rows
+        // 8 kg + r8 for its warp's kg, samples n .. n+15 -- into registers
+        // one step ahead: the loads of step g+1 are in flight while step g
+        // waits for its B buffer and converts.
         const int pw = warp - 1, r8 = lane & 7, c4 = lane >> 3;
-        TcolWalk walk(u0, u1, a.ns);
-        TcolStep st;
+        static_assert(kTcolProdWarps % 2 == 0, "the items of one warp share the half of the slab");
+        const int n = 64 * (pw & 1) + 16 * c4;  // this lane's chunk of the slab
+        constexpr int ITEMS = KG * 2;           // (K group, half of the slab)
+        constexpr int PER = (ITEMS + kTcolProdWarps - 1) / kTcolProdWarps;
+        // loads this lane's items of step q (rows outside the image under
+        // Constant and chunks outside the step's range are left unloaded)
+        auto load = [&](const TcolStep& q, uint4 (&raw)[PER]) {
+            const int n_lo = q.kind == 0 ? kTcolN - 16 * GH : 0;
+            const int n_hi = q.kind == 2 ? 16 * GH : kTcolN;
+            if (n < n_lo || n >= n_hi) return;
+            const int y0 = q.band * kTcolM - K / 2;
+            const int gx = q.slab * kTcolN + n;
+            const bool inside = gx >= 0 && gx + 16 <= a.rowlen;
+            int sx[16];  // in [0, rowlen) or -1 (Constant); read at the image's left and right edges only
+            if (!inside) {
+#pragma unroll
+                for (int e = 0; e < 16; ++e) sx[e] = border_sample(gx + e, a.W, C, a.border);
+            }
+#pragma unroll
+            for (int r = 0; r < PER; ++r) {
+                const int it = pw + r * kTcolProdWarps;
+                if (it >= ITEMS) continue;
+                const int sy = border_index(y0 + 8 * (it >> 1) + r8, a.H, a.border);
+                if (sy < 0) {
+                    const unsigned f = 0x01010101u * a.bvb;
+                    raw[r] = make_uint4(f, f, f, f);
+                } else if (inside) {
+                    raw[r] = __ldg(reinterpret_cast<const uint4*>(a.src + (long long)sy * a.spitch + gx));
+                } else {
+                    raw[r] = tcol_gather16(a, a.src + (long long)sy * a.spitch, sx);
+                }
+            }
+        };
+        TcolWalk walk(u0, u1, a.ns), ahead(u0, u1, a.ns);
+        TcolStep st, sa;
+        uint4 cur[PER];
+        if (ahead.next(sa)) load(sa, cur);
         int g = 0;
         while (walk.next(st)) {
             if (*abort_flag) break;
+            uint4 nxt[PER];
+            if (ahead.next(sa)) load(sa, nxt);
             const int bb = g & 1;
             if (g >= 2 && !tcol_wait(&bempty[bb], (unsigned)((g - 2) >> 1) & 1u, a, abort_flag)) break;
             unsigned char* B = sm + tcol_off_b(bb, K);
-            const int y0 = st.band * kTcolM - K / 2;
-            const int x0 = st.slab * kTcolN;
-            // samples this step needs: the whole slab, or a halo edge
             const int n_lo = st.kind == 0 ? kTcolN - 16 * GH : 0;
             const int n_hi = st.kind == 2 ? 16 * GH : kTcolN;
-            // items: (K group, half of the slab); lane = (row in group, 16-sample chunk of the half)
-            constexpr int ITEMS = KG * 2;
-            constexpr int PER = (ITEMS + kTcolProdWarps - 1) / kTcolProdWarps;
-            uint4 raw[PER];
-            bool fast[PER];
+            if (n >= n_lo && n < n_hi) {
 #pragma unroll
-            for (int r = 0; r < PER; ++r) {
-                const int it = pw + r * kTcolProdWarps;
-                const int kg = it >> 1, half = it & 1;
-                const int n = 64 * half + 16 * c4;
-                fast[r] = false;
-                if (it >= ITEMS || n < n_lo || n >= n_hi) continue;
-                const int sy = border_index(y0 + 8 * kg + r8, a.H, a.border);
-                const int gx = x0 + n;
-                if (sy >= 0 && gx >= 0 && gx + 16 <= a.rowlen) {
-                    raw[r] = __ldg(reinterpret_cast<const uint4*>(a.src + (long long)sy * a.spitch + gx));
-                    fast[r] = true;
+                for (int r = 0; r < PER; ++r) {
+                    const int it = pw + r * kTcolProdWarps;
+                    if (it >= ITEMS) continue;
+                    const int k = 8 * (it >> 1) + r8;
+                    unsigned h[8];
+                    tcol_cvt_word(cur[r].x, h[0], h[1]);
+                    tcol_cvt_word(cur[r].y, h[2], h[3]);
+                    tcol_cvt_word(cur[r].z, h[4], h[5]);
+                    tcol_cvt_word(cur[r].w, h[6], h[7]);
+                    *reinterpret_cast<uint4*>(B + tcol_b_off(n, k)) = make_uint4(h[0], h[1], h[2], h[3]);
+                    *reinterpret_cast<uint4*>(B + tcol_b_off(n + 8, k)) = make_uint4(h[4], h[5], h[6], h[7]);
                 }
-            }
-#pragma unroll
-            for (int r = 0; r < PER; ++r) {
-                const int it = pw + r * kTcolProdWarps;
-                const int kg = it >> 1, half = it & 1;
-                const int n = 64 * half + 16 * c4;
-                if (it >= ITEMS || n < n_lo || n >= n_hi) continue;
-                unsigned h[8];
-                if (fast[r]) {
-                    tcol_cvt_word(raw[r].x, h[0], h[1]);
-                    tcol_cvt_word(raw[r].y, h[2], h[3]);
-                    tcol_cvt_word(raw[r].z, h[4], h[5]);
-                    tcol_cvt_word(raw[r].w, h[6], h[7]);
-                } else {
-                    const int sy = border_index(y0 + 8 * kg + r8, a.H, a.border);
-                    const unsigned char* srow = sy >= 0 ? a.src + (long long)sy * a.spitch : nullptr;
-                    const int gx = x0 + n;
-#pragma unroll
-                    for (int e = 0; e < 8; ++e)
-                        h[e] = (unsigned)tcol_sample_h(a, srow, gx + 2 * e, C) |
-                               ((unsigned)tcol_sample_h(a, srow, gx + 2 * e + 1, C) << 16);
-                }
-                const int k = 8 * kg + r8;
-                *reinterpret_cast<uint4*>(B + tcol_b_off(n, k)) = make_uint4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<uint4*>(B + tcol_b_off(n + 8, k)) = make_uint4(h[4], h[5], h[6], h[7]);
             }
             fence_async_smem();
             mbar_arrive(&bfull[bb]);
+#pragma unroll
+            for (int r = 0; r < PER; ++r) cur[r] = nxt[r];
             ++g;
         }
     } else {
         // ------------------------------------------------------------ row pass
-        const int rw = warp - 1 - kTcolProdWarps;  // 0..7
+        const int rw = warp - 1 - kTcolProdWarps;  // 0 .. kTcolRowWarps-1
         const int q = warp & 3;                    // tensor-memory lane quarter of this warp
-        const int h = rw >> 2;                     // which half of the slab's columns
+        const int h = rw >> 2;                     // which part of the slab's chunks (3, 3 or 2 of 16 columns)
+        const int ch0 = tcol_row_chunk0(h), nch = tcol_row_chunk0(h + 1) - ch0;
         const uint32_t tlane = tbase + ((uint32_t)(32 * q) << 16);
         TcolWalk walk(u0, u1, a.ns);
         TcolStep st, prev{0, 0, 0};
@@ -313,59 +416,42 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
                 // row pass of slab prev (step g-1): buffers g-2, g-1, g
                 const int m = 32 * q + lane;
                 const int y = prev.band * kTcolM + m;
-                const int xs = prev.slab * kTcolN + 64 * h;  // first output sample of this thread
+                const int xs = prev.slab * kTcolN + 16 * ch0;  // first output sample of this thread
                 // column group rg (relative to 64h, in 16s) -> tensor-memory address
                 auto gaddr = [&](int rg) -> uint32_t {
-                    const int col = 64 * h + 16 * rg;  // relative to slab g-1's buffer, may leave [0,128)
+                    const int col = 16 * (ch0 + rg);  // relative to slab g-1's buffer, may leave [0,128)
                     const int dg = col < 0 ? -1 : (col >= kTcolN ? 1 : 0);
                     const int buf = (g - 1 + dg) & 3;
                     return tlane + (uint32_t)(buf * kTcolN + (col - dg * kTcolN));
                 };
-                float v[NG][16];
-                __syncwarp();
-                static_for<0, 2 * GH + 1>([&](auto I) {
-                    constexpr int i = decltype(I)::value;
-                    tcol_ld16(gaddr(i - GH), v[i]);
-                });
-                static_for<0, 2 * GH + 1>([&](auto I) { tcol_ld_wait(v[decltype(I)::value]); });
                 unsigned char* drow = a.dst + (long long)y * a.dpitch;
                 const bool row_ok = y < a.H;
-                static_for<0, 4>([&](auto J) {
-                    constexpr int j = decltype(J)::value;
-                    // prefetch the group chunk j+1 needs last
+                // this warp's chunks of 16 outputs, one compiled body: the chunk's
+                // window (its 16 columns and GH groups either side) is read
+                // from tensor memory afresh, so the loop stays small enough
+                // for the instruction cache
+#pragma unroll 1
+                for (int j = 0; j < nch; ++j) {
+                    float v[NG][16];
                     __syncwarp();
-                    if constexpr (j + GH + 1 < 4 + GH) tcol_ld16(gaddr(j + GH + 1), v[j + 2 * GH + 1]);
+                    static_for<0, NG>([&](auto I) {
+                        constexpr int i = decltype(I)::value;
+                        tcol_ld16(gaddr(j + i - GH), v[i]);
+                    });
+                    static_for<0, NG>([&](auto I) { tcol_ld_wait(v[decltype(I)::value]); });
                     unsigned words[4];
-#pragma unroll
-                    for (int t4 = 0; t4 < 4; ++t4) {
-                        unsigned wd = 0;
-#pragma unroll
-                        for (int t = 0; t < 4; ++t) {
-                            const int o = 16 * j + 4 * t4 + t;  // output, relative to 64h
-                            float acc = a.off;
-#pragma unroll
-                            for (int i = 0; i < K; ++i) {
-                                const int col = o + C * (i - K / 2) + 16 * GH;  // into v, group 0 = rg -GH
-                                acc = fmaf(a.kx[i], v[col >> 4][col & 15], acc);
-                            }
-                            if (a.clamp) acc = fminf(fmaxf(acc, 0.f), 255.f);
-                            const float r = __fadd_rd(acc, 8388608.0f);
-                            wd = __byte_perm(wd, __float_as_uint(r), byte_insert_sel(t));
-                        }
-                        words[t4] = wd;
-                    }
+                    tcol_row_chunk<K, C, GH>(a, v, words);
                     const int xo = xs + 16 * j;
                     if (row_ok && xo < a.rowlen) {
                         if (a.vec_store && xo + 16 <= a.rowlen) {
                             *reinterpret_cast<uint4*>(drow + xo) = make_uint4(words[0], words[1], words[2], words[3]);
                         } else {
-                            for (int e = 0; e < 16 && xo + e < a.rowlen; ++e)
-                                drow[xo + e] = (unsigned char)(words[e >> 2] >> (8 * (e & 3)));
+#pragma unroll
+                            for (int e = 0; e < 16; ++e)
+                                if (xo + e < a.rowlen) drow[xo + e] = (unsigned char)(words[e >> 2] >> (8 * (e & 3)));
                         }
                     }
-                    __syncwarp();
-                    if constexpr (j + GH + 1 < 4 + GH) tcol_ld_wait(v[j + 2 * GH + 1]);
-                });
+                }
                 (void)R;
             }
             // buffers no longer read: step g-2 when it belongs to this run, and
@@ -440,7 +526,7 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
     if (!sep_tcol_supported(K, C)) return false;
     if (((uintptr_t)src & 15) || (spitch & 15) || spitch <= 0 || spitch >= (1LL << 40)) return false;
     if (dpitch <= 0 || dpitch >= (1LL << 40)) return false;
-    if (border == IPFC_BORDER_CONSTANT && !(bv == std::floor(bv) && std::fabs(bv - 128.0) <= 2048.0)) return false;
+    if (border == IPFC_BORDER_CONSTANT && !(bv == std::floor(bv) && bv >= 0.0 && bv <= 255.0)) return false;
     double mx = 0, sy = 0, sx = 0;
     for (int j = 0; j < K; ++j) {
         if (!std::isfinite(ky[j]) || !std::isfinite(kx[j])) return false;
@@ -464,7 +550,7 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
     a.H = H;
     a.rowlen = W * C;
     a.border = border;
-    a.bvh = __half_as_ushort(__double2half(border == IPFC_BORDER_CONSTANT ? bv - 128.0 : 0.0));
+    a.bvb = border == IPFC_BORDER_CONSTANT ? (unsigned)bv : 0u;
     a.nb = (H + kTcolM - 1) / kTcolM;
     a.ns = (a.rowlen + kTcolN - 1) / kTcolN;
     a.units = a.nb * a.ns;
@@ -478,7 +564,10 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
         const __half lo = __double2half(w - (double)__half2float(hi));
         a.ahi[j] = __half_as_ushort(hi);
         a.alo[j] = __half_as_ushort(lo);
-        a.kx[j] = std::ldexp((float)kx[j], -ex);
+        const float kxs = std::ldexp((float)kx[j], -ex);
+        unsigned kb = 0;
+        std::memcpy(&kb, &kxs, sizeof(kb));
+        a.kx2[j] = ((unsigned long long)kb << 32) | kb;
     }
     a.err = device_error_word();
     cudaError_t e = cudaErrorInvalidValue;

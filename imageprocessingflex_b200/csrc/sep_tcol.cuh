@@ -41,8 +41,11 @@ namespace ipfc {
 constexpr int kTcolM = 128;                   // output rows per band (MMA M)
 constexpr int kTcolN = 128;                   // samples per slab (MMA N)
 constexpr int kTcolMaxK = 31;
-constexpr int kTcolProdWarps = 4;             // convert uint8 rows into B
-constexpr int kTcolRowWarps = 8;              // row pass (2 per tensor-memory lane quarter)
+constexpr int kTcolProdWarps = 6;             // convert uint8 rows into B
+constexpr int kTcolRowWarps = 12;             // row pass (3 per tensor-memory lane quarter)
+// The 8 chunks of 16 columns of a slab, split 3 / 3 / 2 among the three
+// row-pass warps of a lane quarter: first chunk of part p.
+__host__ __device__ constexpr int tcol_row_chunk0(int p) { return p <= 0 ? 0 : p == 1 ? 3 : p == 2 ? 6 : 8; }
 constexpr int kTcolThreads = 32 * (1 + kTcolProdWarps + kTcolRowWarps);
 constexpr int kTcolTmemCols = 4 * kTcolN;     // four slab buffers
 constexpr int kTcolKGroupBytes = 2048;        // 16 core matrices of 128 B
@@ -51,11 +54,22 @@ constexpr int kTcolKGroupBytes = 2048;        // 16 core matrices of 128 B
 __host__ __device__ constexpr int tcol_kr(int K) { return (kTcolM + K - 1 + 15) / 16 * 16; }
 // One operand (A_hi, A_lo or one B buffer) in bytes.
 __host__ __device__ constexpr int tcol_operand_bytes(int K) { return tcol_kr(K) / 8 * kTcolKGroupBytes; }
-// Shared layout: A_hi, A_lo, B[0], B[1], then 12 mbarriers.
+// Raw source bytes of one step as copied from the image (KR rows x 128
+// samples); kTcolStages of them let the copies run two steps ahead.
+constexpr int kTcolStages = 0;
+__host__ __device__ constexpr int tcol_stage_bytes(int K) { return tcol_kr(K) * kTcolN; }
+// Shared layout: A_hi, A_lo, B[0], B[1], the stages, then 13 mbarriers, the
+// abort flag and the tensor-memory slot (128 bytes), then the FP16 taps
+// (2 x 32).
 __host__ __device__ constexpr int tcol_off_a(int hl, int K) { return hl * tcol_operand_bytes(K); }
 __host__ __device__ constexpr int tcol_off_b(int b, int K) { return (2 + b) * tcol_operand_bytes(K); }
-__host__ __device__ constexpr int tcol_off_bar(int K) { return 4 * tcol_operand_bytes(K); }
-__host__ __device__ constexpr int tcol_smem(int K) { return tcol_off_bar(K) + 128; }
+__host__ __device__ constexpr int tcol_off_s(int st, int K) { return 4 * tcol_operand_bytes(K) + st * tcol_stage_bytes(K); }
+__host__ __device__ constexpr int tcol_off_bar(int K) { return tcol_off_s(kTcolStages, K); }
+__host__ __device__ constexpr int tcol_smem(int K) { return tcol_off_bar(K) + 256; }
+// Byte offset of the 16-sample chunk at sample n (a multiple of 16) of
+// staged row k: chunks XOR-swizzled by the row so that the 8 rows a
+// quarter-warp reads at one n fall in distinct banks.
+__host__ __device__ constexpr int tcol_s_off(int k, int n) { return k * kTcolN + (((n >> 4) ^ (k & 7)) << 4); }
 
 __host__ __device__ inline int tcol_a_off(int m, int k) {
     return (m >> 3) * 128 + (k >> 3) * kTcolKGroupBytes + (m & 7) * 16 + (k & 7) * 2;
