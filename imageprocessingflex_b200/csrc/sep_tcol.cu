@@ -47,6 +47,7 @@ cudaError_t ensure_smem_attr(const void* func, int bytes, unsigned* done_mask);
 
 constexpr unsigned kErrTcolWait = 0x301u;   // a pipeline wait gave up
 constexpr unsigned kErrTcolDrain = 0x302u;  // the final MMA drain gave up: tensor memory left allocated
+constexpr int kTcolMaxCtas = 160;           // balanced unit split passed by value up to this grid
 
 struct TcolArgs {
     const unsigned char* src;
@@ -64,6 +65,8 @@ struct TcolArgs {
     unsigned short ahi[kTcolMaxK + 1], alo[kTcolMaxK + 1];  // FP16 bits of ky * 2^e (hi, lo)
     unsigned long long kx2[kTcolMaxK + 1];                   // kx * 2^-e in both FP32 lanes
     unsigned* err;
+    int nsplit;                      // > 0: CTA b walks units split[b] .. split[b+1]-1
+    int split[kTcolMaxCtas + 1];
 };
 
 namespace {
@@ -276,8 +279,8 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
     tc_fence_after();
     const uint32_t tbase = *tslot;
 
-    const int u0 = (int)((long long)blockIdx.x * a.units / gridDim.x);
-    const int u1 = (int)((long long)(blockIdx.x + 1) * a.units / gridDim.x);
+    const int u0 = a.nsplit ? a.split[blockIdx.x] : (int)((long long)blockIdx.x * a.units / gridDim.x);
+    const int u1 = a.nsplit ? a.split[blockIdx.x + 1] : (int)((long long)(blockIdx.x + 1) * a.units / gridDim.x);
 
     if (warp == 0) {
         // ------------------------------------------------------------ MMA issue
@@ -485,8 +488,36 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
 
 namespace {
 
+// Splits the (band, slab) units into `grid` contiguous ranges of about
+// equal cost.  A unit costs one step; the last slab of a band also pays for
+// the right halo at the image's edge, whose border-resolved gathers take
+// about as long as kTcolEdgeCost slab steps (measured), and every range
+// pays its own left and right halo steps.
+constexpr double kTcolEdgeCost = 2.5;
+constexpr double kTcolHaloCost = 0.3;
+void tcol_split(TcolArgs& a, int grid) {
+    auto cost = [&](int u) { return 1.0 + (u % a.ns == a.ns - 1 ? kTcolEdgeCost : 0.0); };
+    double total = 0;
+    for (int u = 0; u < a.units; ++u) total += cost(u);
+    total += 2 * kTcolHaloCost * grid;
+    const double share = total / grid;
+    a.nsplit = grid;
+    a.split[0] = 0;
+    int u = 0;
+    double done = 0;  // cost of the units before u, with the halos of the ranges so far
+    for (int b = 1; b < grid; ++b) {
+        done += 2 * kTcolHaloCost;
+        // range b-1 ends where the running cost is nearest b shares; at
+        // least one unit per range, and one left for each range after it
+        while (u < a.units - (grid - b) &&
+               (a.split[b - 1] == u || done + 0.5 * cost(u) <= b * share)) done += cost(u++);
+        a.split[b] = u;
+    }
+    a.split[grid] = a.units;
+}
+
 template <int K, int C>
-cudaError_t tcol_launch_kc(const TcolArgs& a, cudaStream_t s) {
+cudaError_t tcol_launch_kc(TcolArgs a, cudaStream_t s) {
     static unsigned done = 0;
     cudaError_t e = ensure_smem_attr((const void*)sep_tcol_kernel<K, C>, tcol_smem(K), &done);
     if (e != cudaSuccess) return e;
@@ -494,6 +525,7 @@ cudaError_t tcol_launch_kc(const TcolArgs& a, cudaStream_t s) {
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     const int grid = a.units < sms ? a.units : sms;
+    if (grid <= kTcolMaxCtas) tcol_split(a, grid);
     sep_tcol_kernel<K, C><<<grid, kTcolThreads, tcol_smem(K), s>>>(a);
     return cudaGetLastError();
 }
