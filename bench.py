@@ -48,7 +48,7 @@ METRIC = "Mpix/s plain vs batched/served at <=1 LSB; p50/p99 latency; % HBM roof
 UNIT = "Mpix/s"
 WORKLOAD = "gaussianBlur sigma=2 (13 taps) Reflect101, 3840x2160x3 uint8 -> uint8"
 FALLBACK_HBM_GBS = 6650.0
-PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "sep_gaussian_4k_rgb_u8.md")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "sep_tcol_4k_rgb_u8.md")
 
 
 def parse_args():
@@ -373,7 +373,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                         else "fallback 6.65 TB/s", "kernel": "sep_fused u8 C=3 13x13",
+                         else "fallback 6.65 TB/s", "kernel": "sep_tcol_kernel<13, 3> (tcgen05 column pass)",
                          "alg_bytes_per_launch": int(alg_bytes), "ms_per_launch": round(ms_per_launch, 5)},
             "clocks": clk.summary(),
         }

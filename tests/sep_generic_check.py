@@ -1,9 +1,10 @@
 """Replays the separable golden cases (gaussian, sep, sobel) through the CUDA
 library and exits non-zero on any parity failure.  Run by
 test_gpu_parity.test_generic_separable_path with IPFC_SEP_PATH=generic (the
-generic fused / two-pass kernels) and by test_tcol_separable_path with
-IPFC_SEP_PATH=tcol (the tensor-core column-pass kernel), so those kernels
-are checked as well as the default one.  With --fullsize it also checks
+generic fused / two-pass kernels), by test_tcol_separable_path with
+IPFC_SEP_PATH=tcol (the tensor-core column-pass kernel) and by
+test_cuda_core_separable_path_at_full_size with IPFC_SEP_PATH=fast (the
+CUDA-core kernel), so each kernel is checked whichever the default picks.  With --fullsize it also checks
 gaussianBlur sigma=2 on 1920x1080x3 and 3840x2160x3 uint8 within 1 LSB.
 With --sweep it also runs uint8 sepFilter2D over awkward shapes (1x1,
 widths and heights that are no multiple of the kernels' tiles), 1, 3 and 4

@@ -274,6 +274,22 @@ def test_tcol_separable_path(gpu):
     print(r.stdout)
 
 
+def test_cuda_core_separable_path_at_full_size(gpu):
+    """The CUDA-core fast kernel, which large uint8 images leave for the
+    tensor-core kernel by default, kept on for every call (IPFC_SEP_PATH=fast):
+    the golden cases and the full-size uint8 Gaussians."""
+    import os
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    env = dict(os.environ, IPFC_SEP_PATH="fast")
+    r = subprocess.run([sys.executable, os.path.join(here, "sep_generic_check.py"), "--fullsize"], env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    assert "separable cases ok (fast path)" in r.stdout and "3840x2160x3 ok" in r.stdout
+
+
 @pytest.mark.parametrize("c", [1, 3, 4])
 @pytest.mark.parametrize("w", [1200, 1201])
 def test_medium_all_borders_u8(gpu, orc, c, w):
