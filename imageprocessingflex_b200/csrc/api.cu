@@ -320,6 +320,12 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
 // keeps uint8 calls off the tensor cores; =tcol takes the tensor-core kernel
 // for every size it covers.
 constexpr long long kTcolMinSamples = 1LL << 22;
+// Callers that share the GPU among many streams (the request server) keep
+// separable calls on the CUDA-core kernel: the tensor-core kernel is
+// persistent, one CTA with 203 KB of shared memory on every SM, so while it
+// runs no other stream's kernel gets an SM.
+static thread_local bool t_shared_gpu = false;
+void set_shared_gpu(bool on) { t_shared_gpu = on; }
 static int sep_path_mode() {
     static const int mode = [] {  // read once, thread-safe initialisation
         const char* v = std::getenv("IPFC_SEP_PATH");
@@ -420,7 +426,8 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
                             &f))
         return false;
     const int mode = sep_path_mode();
-    const bool tcol = mode == 4 || (mode == 0 && (long long)src->width * src->channels * src->height >= kTcolMinSamples);
+    const bool tcol = mode == 4 || (mode == 0 && !t_shared_gpu &&
+                                    (long long)src->width * src->channels * src->height >= kTcolMinSamples);
     if (tcol && src->dtype == IPFC_U8 && dst->dtype == IPFC_U8 &&
         sep_tcol_launch(in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, kx, ky, kw,
                         border, delta, bv, f.clamp, s, e))

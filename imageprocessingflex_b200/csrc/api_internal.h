@@ -24,6 +24,9 @@ int take_device_error(cudaStream_t s, const char* fn);
 // Checks a source/destination pair: IPFC_OK, an error, or -1 for an empty
 // image (nothing to do).
 int check_pair(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type);
+// Per thread: calls from this thread run on kernels that leave SMs to other
+// streams (the request server sets it around its requests).
+void set_shared_gpu(bool on);
 int check_pair_resized(const ipfc_image* src, const ipfc_image* dst, const char* fn, bool same_type);
 
 // A device view of an image: the caller's memory, or a staged copy.

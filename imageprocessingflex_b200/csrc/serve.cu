@@ -44,6 +44,7 @@
 
 namespace ipfc {
 int set_error(int code, const char* fmt, ...);
+void set_shared_gpu(bool on);
 int cuda_status(cudaError_t e, const char* fn);
 size_t elem_bytes(int dt);
 int gaussian_taps(double sigma, int ksize, std::vector<double>& k);
@@ -221,6 +222,11 @@ bool batch_item(const Req& q, HostItem* h) {
 
 // Runs one non-batched request through its per-image entry point.
 int run_single(const Req& q, cudaStream_t st) {
+    // leave SMs to the other streams' requests (no persistent whole-GPU kernel)
+    struct SharedGpu {
+        SharedGpu() { set_shared_gpu(true); }
+        ~SharedGpu() { set_shared_gpu(false); }
+    } shared_gpu;
     const ipfc_request& r = q.r;
     ipfc_image sv = r.src, dv = r.dst;
     sv.data = q.dsrc;
