@@ -61,7 +61,15 @@ cudaError_t morph_typed(const MorphArgs& a, cudaStream_t s) {
 
 }  // namespace
 
+bool morph3_stream_launch(const MorphCore& a, cudaStream_t s, cudaError_t* e);
+
 cudaError_t morph_launch(int dt, const MorphArgs& a, cudaStream_t s) {
+    // uint8, the 3 x 3 element with 16-byte aligned rows: the streaming
+    // kernel (morph3_stream.cu), no shared-memory staging
+    if (dt == IPFC_U8) {
+        cudaError_t e = cudaSuccess;
+        if (morph3_stream_launch(a, s, &e)) return e;
+    }
     // uint8 rectangles: the packed-byte tile's direct scans up to 9 members
     // per axis; longer ones run van Herk / Gil-Werman in the generic tile
     if (dt == IPFC_U8 && a.is_rect && a.sw < kMorphU8VhgwFrom && a.sh < kMorphU8VhgwFrom &&
