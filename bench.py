@@ -74,7 +74,9 @@ def parse_args():
                     choices=["headline", "batch", "serve", "filter2d", "sep_sweep", "erode", "median3", "median5"],
                     help="headline: 4K RGB gaussianBlur (the driver's line); batch: 512-image uneven mix, "
                          "batched vs plain per-image launches; serve: Poisson request stream through the "
-                         "continuous-batching server vs one request at a time")
+                         "continuous-batching server vs one request at a time; filter2d: FP32 vs split forms; "
+                         "sep_sweep: f32 separable and Sobel sweep; erode, median3, median5: per-image calls "
+                         "on 4K RGB (with --launches-only N: the profiling programs)")
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-rate", type=float, default=3000.0, help="arrivals per second")
     ap.add_argument("--serve-seed", type=int, default=77)
@@ -1057,6 +1059,9 @@ def run_neighbourhood_op(args):
 
     from imageprocessingflex_b200 import _lib
 
+    if not torch.cuda.is_available():
+        print(f"bench.py: --workload {args.workload} needs a GPU", file=sys.stderr)
+        return 2
     lib = _lib.load()
     dev = torch.device("cuda", torch.cuda.current_device())
     host = seeded_image(W_IMG, H_IMG, C_IMG)

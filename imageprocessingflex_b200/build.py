@@ -53,7 +53,7 @@ def _stale(target: str, deps) -> bool:
 
 def _compile(src: str, obj: str, verbose: bool) -> None:
     cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
-    if os.path.basename(src).startswith(("sep_fast_", "batch_")):
+    if os.path.basename(src).startswith(("sep_fast_", "batch_", "sep_tcol")):
         cmd.insert(1, "--split-compile=4")  # many kernels or tile functions per file: compile them in parallel
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

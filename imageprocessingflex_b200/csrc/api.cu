@@ -313,9 +313,10 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
 
 // Kernel selection for separable filters.  Default: uint8 -> uint8 calls on
 // images of at least kTcolMinSamples samples that the tensor-core
-// column-pass kernel covers (sep_tcol.cu) run there -- 1.34x faster than the
-// CUDA-core kernel on 3840x2160x3 -- and the rest on the CUDA-core fast
-// kernel where it is instantiated, else on the generic kernels.
+// column-pass kernel covers (sep_tcol.cu) run there where it is the faster
+// one (from 9 taps on 3 or 4 channels, from 15 on one channel; gaussianBlur
+// sigma 2 on 3840x2160x3: 1.34x), the rest on the CUDA-core fast kernel
+// where it is instantiated, else on the generic kernels.
 // IPFC_SEP_PATH=generic forces the generic fused/two-pass kernels; =fast
 // keeps uint8 calls off the tensor cores; =tcol takes the tensor-core kernel
 // for every size it covers.
@@ -426,7 +427,12 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
                             &f))
         return false;
     const int mode = sep_path_mode();
-    const bool tcol = mode == 4 || (mode == 0 && !t_shared_gpu &&
+    // measured on 3840x2160 (µs per image, CUDA-core / tensor-core): C = 3 --
+    // K 7: 49.4 / 51.6, K 9: 57.9 / 52.3, K 13: 63.8 / 54.9; C = 1 -- K 13:
+    // 28.9 / 31.8, K 15: 33.8 / 32.5.  The tensor-core kernel's cost barely
+    // depends on K, the CUDA-core kernel's grows with it.
+    const bool tcol_wins = kw >= (src->channels == 1 ? 15 : 9);
+    const bool tcol = mode == 4 || (mode == 0 && !t_shared_gpu && tcol_wins &&
                                     (long long)src->width * src->channels * src->height >= kTcolMinSamples);
     if (tcol && src->dtype == IPFC_U8 && dst->dtype == IPFC_U8 &&
         sep_tcol_launch(in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, kx, ky, kw,

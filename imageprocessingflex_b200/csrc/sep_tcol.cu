@@ -48,6 +48,7 @@ cudaError_t ensure_smem_attr(const void* func, int bytes, unsigned* done_mask);
 constexpr unsigned kErrTcolWait = 0x301u;   // a pipeline wait gave up
 constexpr unsigned kErrTcolDrain = 0x302u;  // the final MMA drain gave up: tensor memory left allocated
 constexpr int kTcolMaxCtas = 160;           // balanced unit split passed by value up to this grid
+constexpr int kTcolMaxBuiltK = 15;          // odd K from 3 up to this are instantiated (KR = 144 rows)
 
 struct TcolArgs {
     const unsigned char* src;
@@ -532,20 +533,33 @@ cudaError_t tcol_launch_kc(TcolArgs a, cudaStream_t s) {
 
 template <int K>
 bool tcol_launch_k(int C, const TcolArgs& a, cudaStream_t s, cudaError_t* e) {
-    if (C == 1) *e = tcol_launch_kc<K, 1>(a, s);
-    else if (C == 3) *e = tcol_launch_kc<K, 3>(a, s);
-    else if (C == 4) *e = tcol_launch_kc<K, 4>(a, s);
-    else return false;
-    return true;
+    if (C == 1) {
+        *e = tcol_launch_kc<K, 1>(a, s);
+        return true;
+    }
+    if constexpr (3 * (K / 2) <= 32) {
+        if (C == 3) {
+            *e = tcol_launch_kc<K, 3>(a, s);
+            return true;
+        }
+    }
+    if constexpr (4 * (K / 2) <= 32) {
+        if (C == 4) {
+            *e = tcol_launch_kc<K, 4>(a, s);
+            return true;
+        }
+    }
+    return false;
 }
 
 }  // namespace
 
-// (K, C) combinations instantiated: the row pass reaches at most 32 columns
-// either side (C * (K/2) <= 32).
+// (K, C) combinations instantiated: odd K from 3 to 15 (144 staged rows; from
+// 17 taps the 160-row band's producer registers spill) with C in {1, 3, 4}
+// while the row pass reaches at most 32 columns either side (C * (K/2) <= 32).
 bool sep_tcol_supported(int K, int C) {
     if (!(C == 1 || C == 3 || C == 4)) return false;
-    if (!(K == 5 || K == 13)) return false;
+    if (K < 3 || K > kTcolMaxBuiltK || (K & 1) == 0) return false;
     return C * (K / 2) <= 32;
 }
 
@@ -605,8 +619,13 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
     cudaError_t e = cudaErrorInvalidValue;
     bool launched = false;
     switch (K) {
+        case 3: launched = tcol_launch_k<3>(C, a, s, &e); break;
         case 5: launched = tcol_launch_k<5>(C, a, s, &e); break;
+        case 7: launched = tcol_launch_k<7>(C, a, s, &e); break;
+        case 9: launched = tcol_launch_k<9>(C, a, s, &e); break;
+        case 11: launched = tcol_launch_k<11>(C, a, s, &e); break;
         case 13: launched = tcol_launch_k<13>(C, a, s, &e); break;
+        case 15: launched = tcol_launch_k<15>(C, a, s, &e); break;
         default: return false;
     }
     if (!launched) return false;

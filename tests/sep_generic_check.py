@@ -8,7 +8,7 @@ CUDA-core kernel), so each kernel is checked whichever the default picks.  With 
 gaussianBlur sigma=2 on 1920x1080x3 and 3840x2160x3 uint8 within 1 LSB.
 With --sweep it also runs uint8 sepFilter2D over awkward shapes (1x1,
 widths and heights that are no multiple of the kernels' tiles), 1, 3 and 4
-channels, 5 and 13 taps (non-negative and signed), every border (Constant
+channels, every odd tap count from 3 to 15 (non-negative and signed), every border (Constant
 with an integer border value) against the oracle within 1 LSB."""
 import os
 import sys
@@ -58,7 +58,9 @@ def sweep():
     for c in (1, 3, 4):
         for w, h in shapes:
             img = oracle.random_image(w, h, c, np.uint8, 31 * w + h + c)
-            for k in (5, 13):
+            for k in (3, 5, 7, 9, 11, 13, 15):
+                if c * (k // 2) > 32:
+                    continue
                 for signed in (False, True):
                     kx = rng.random(k) + (-0.3 if signed else 0.0)
                     ky = rng.random(k) + (-0.3 if signed else 0.0)
