@@ -67,7 +67,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="leave the shortened filter2D / batch / serve measurements out of the default line")
-    ap.add_argument("--extras-serve-requests", type=int, default=3000)
+    ap.add_argument("--extras-serve-requests", type=int, default=6000)
     ap.add_argument("--launches-only", type=int, default=0,
                     help="run this many launches of the workload on one resident image and exit (for ncu captures)")
     ap.add_argument("--workload", default="headline",
