@@ -205,6 +205,20 @@ def test_fullsize_gaussian_u8_rgb(gpu, orc):
         assert rate < 1e-4
 
 
+@pytest.mark.parametrize("c", [1, 3, 4])
+def test_fullsize_gaussian_u8_every_tap_count(gpu, orc, c):
+    """gaussianBlur on 3840x2160 uint8 at sigmas giving 3, 7, 9, 11 and 15
+    taps, 1, 3 and 4 channels: the default path (tensor-core kernel from 9 taps
+    on 3 or 4 channels and 15 on one, the CUDA-core kernel below) within 1 LSB,
+    mismatch rate below 1e-4."""
+    img = oracle.random_image(3840, 2160, c, np.uint8, 20 + c)
+    for sigma in (0.4, 1.0, 1.4, 1.7, 2.4):
+        got = gpu.gaussianBlur(img, sigma)
+        want = orc.gaussian_blur(img, sigma)
+        rate = _lsb_report(got, want, f"gaussian sigma {sigma} 3840x2160x{c}")
+        assert rate < 1e-4
+
+
 def test_fullsize_sobel_int16_exact(gpu, orc):
     img = oracle.random_image(3840, 2160, 1, np.uint8, 2)
     for ksize in (3, 5):
