@@ -489,32 +489,9 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
 
 namespace {
 
-// Splits the (band, slab) units into `grid` contiguous ranges of about
-// equal cost.  A unit costs one step; the last slab of a band also pays for
-// the right halo at the image's edge, whose border-resolved gathers take
-// about as long as kTcolEdgeCost slab steps (measured), and every range
-// pays its own left and right halo steps.
-constexpr double kTcolEdgeCost = 2.5;
-constexpr double kTcolHaloCost = 0.3;
 void tcol_split(TcolArgs& a, int grid) {
-    auto cost = [&](int u) { return 1.0 + (u % a.ns == a.ns - 1 ? kTcolEdgeCost : 0.0); };
-    double total = 0;
-    for (int u = 0; u < a.units; ++u) total += cost(u);
-    total += 2 * kTcolHaloCost * grid;
-    const double share = total / grid;
     a.nsplit = grid;
-    a.split[0] = 0;
-    int u = 0;
-    double done = 0;  // cost of the units before u, with the halos of the ranges so far
-    for (int b = 1; b < grid; ++b) {
-        done += 2 * kTcolHaloCost;
-        // range b-1 ends where the running cost is nearest b shares; at
-        // least one unit per range, and one left for each range after it
-        while (u < a.units - (grid - b) &&
-               (a.split[b - 1] == u || done + 0.5 * cost(u) <= b * share)) done += cost(u++);
-        a.split[b] = u;
-    }
-    a.split[grid] = a.units;
+    tcol_split_units(a.units, a.ns, grid, a.split);
 }
 
 template <int K, int C>

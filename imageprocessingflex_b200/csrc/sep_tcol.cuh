@@ -135,4 +135,32 @@ struct TcolWalk {
     }
 };
 
+// Splits the (band, slab) units into `grid` contiguous ranges of about
+// equal cost: split[b] .. split[b+1]-1 is range b (split has grid + 1
+// entries).  A unit costs one step; the last slab of a band also pays for
+// the right halo at the image's edge, whose border-resolved gathers take
+// about as long as kTcolEdgeCost slab steps (measured), and every range pays
+// its own left and right halo steps.  Every range gets at least one unit
+// (grid <= units).
+constexpr double kTcolEdgeCost = 2.5;
+constexpr double kTcolHaloCost = 0.3;
+inline void tcol_split_units(int units, int ns, int grid, int* split) {
+    auto cost = [&](int u) { return 1.0 + (u % ns == ns - 1 ? kTcolEdgeCost : 0.0); };
+    double total = 0;
+    for (int u = 0; u < units; ++u) total += cost(u);
+    total += 2 * kTcolHaloCost * grid;
+    const double share = total / grid;
+    split[0] = 0;
+    int u = 0;
+    double done = 0;  // cost of the units before u, with the halos of the ranges so far
+    for (int b = 1; b < grid; ++b) {
+        done += 2 * kTcolHaloCost;
+        // range b-1 ends where the running cost is nearest b shares; at
+        // least one unit per range, and one left for each range after it
+        while (u < units - (grid - b) && (split[b - 1] == u || done + 0.5 * cost(u) <= b * share)) done += cost(u++);
+        split[b] = u;
+    }
+    split[grid] = units;
+}
+
 }  // namespace ipfc

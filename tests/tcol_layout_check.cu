@@ -16,7 +16,9 @@
 // sum_j (hi_j + lo_j) B[n][m + j] for every (m, n), for slab and halo steps
 // and every K the kernel is built for.  It also walks TcolWalk for many
 // (units, CTAs, slabs per band) and checks that every unit is a slab step
-// exactly once, bracketed by halo steps of its own band.
+// exactly once, bracketed by halo steps of its own band, and that the
+// host's cost-balanced split of the units (tcol_split_units) is contiguous,
+// never empty and within two edge units of the average cost.
 //
 // Prints "ok <cases>" and exits 0, or the first failures and exits 1.
 #include <cstdint>
@@ -140,6 +142,31 @@ static void check_k(int K, std::mt19937& rng) {
     }
 }
 
+// The host's cost-balanced unit split: contiguous, every range non-empty,
+// and no range costing more than the average share plus one edge unit and
+// its halos (the split's granularity).
+static void check_split(std::mt19937& rng) {
+    for (int t = 0; t < 3000; ++t) {
+        const int nb = 1 + (int)(rng() % 40), ns = 1 + (int)(rng() % 120);
+        const int units = nb * ns;
+        const int grid = 1 + (int)(rng() % std::min(units, 160));
+        std::vector<int> split(grid + 1, -1);
+        tcol_split_units(units, ns, grid, split.data());
+        double total = 2 * kTcolHaloCost * grid, worst = 0;
+        auto cost = [&](int u) { return 1.0 + (u % ns == ns - 1 ? kTcolEdgeCost : 0.0); };
+        for (int u = 0; u < units; ++u) total += cost(u);
+        if (split[0] != 0 || split[grid] != units) fail("split ends", split[0], split[grid], units);
+        for (int b = 0; b < grid; ++b) {
+            if (split[b + 1] <= split[b]) fail("empty or reversed range", b, split[b], split[b + 1]);
+            double c = 2 * kTcolHaloCost;
+            for (int u = split[b]; u < split[b + 1]; ++u) c += cost(u);
+            worst = std::max(worst, c);
+        }
+        ++cases;
+        if (worst > total / grid + 2 * (1.0 + kTcolEdgeCost) + 1e-9) fail("unbalanced split", units, grid, (int)worst);
+    }
+}
+
 static void check_walk(std::mt19937& rng) {
     for (int t = 0; t < 3000; ++t) {
         const int nb = 1 + (int)(rng() % 20), ns = 1 + (int)(rng() % 100);
@@ -179,6 +206,7 @@ static void check_walk(std::mt19937& rng) {
 int main() {
     std::mt19937 rng(12345);
     for (int K : {3, 5, 7, 9, 11, 13, 15, 17, 21, 25, 31}) check_k(K, rng);
+    check_split(rng);
     check_walk(rng);
     if (bad) {
         std::printf("%lld failures\n", bad);
