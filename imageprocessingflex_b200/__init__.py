@@ -26,7 +26,9 @@ from .filters import (  # noqa: F401
     gaussianBlur,
     gaussianKernel1D,
     getStructuringElement,
+    gradientMagnitude,
     integralImage,
+    laplacian,
     medianBlur,
     morphologyEx,
     pyrDown,
@@ -34,6 +36,7 @@ from .filters import (  # noqa: F401
     sepFilter2D,
     sobel,
     ssim,
+    unsharpMask,
 )
 
 __version__ = "1.0.0"

@@ -88,6 +88,9 @@ _SIGNATURES = {
     "ipfc_corner_harris": (c_int, [IMG_P, IMG_P, c_int, c_int, c_double, c_void_p]),
     "ipfc_corner_min_eigen_val": (c_int, [IMG_P, IMG_P, c_int, c_int, c_void_p]),
     "ipfc_canny": (c_int, [IMG_P, IMG_P, c_double, c_double, c_int, c_int, c_void_p]),
+    "ipfc_laplacian": (c_int, [IMG_P, IMG_P, c_int, c_double, c_int, c_void_p]),
+    "ipfc_gradient_magnitude": (c_int, [IMG_P, IMG_P, c_int, c_void_p]),
+    "ipfc_unsharp_mask": (c_int, [IMG_P, IMG_P, c_double, c_double, c_double, c_void_p]),
     "ipfc_erode": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_void_p]),
     "ipfc_dilate": (c_int, [IMG_P, IMG_P, c_void_p, c_int, c_int, c_int, c_void_p]),
     "ipfc_batch_create": (c_int, [c_void_p]),

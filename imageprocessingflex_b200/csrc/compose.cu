@@ -5,6 +5,7 @@
 //   integralImage      (include/ipf/filter.hpp:527-541)
 //   adaptiveThreshold  (include/ipf/filter.hpp:554-567)
 //   pyrDown / pyrUp    (include/ipf/geometry.hpp:504-525)
+//   laplacian, gradientMagnitude, unsharpMask (include/ipf/filter.hpp:426-483)
 // Intermediates live in stream-ordered device buffers; host images are staged
 // once in and once out.  Wherever the reference computes in FP64 these
 // kernels do too, in its operation order with separately rounded products
@@ -579,6 +580,177 @@ extern "C" int ipfc_pyr_up(const ipfc_image* src, ipfc_image* dst, void* stream)
         const ipfc_image vu = dev_image(up.p, 2 * W, 2 * H, C, IPFC_F64, up.pitch);
         ipfc_image vo = dev_image(out.ptr, 2 * W, 2 * H, C, src->dtype, out.pitch);
         rc = run_sep(&vu, &vo, k, 5, k, 5, -1, -1, IPFC_BORDER_REFLECT101, 0.0, 0.0, s, fn, true);
+    }
+    const int frc = finish(dst, &in, &out, s, fn);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    return frc;
+}
+
+// ---------------------------------------------------------------------------
+// laplacian, gradientMagnitude, unsharpMask (include/ipf/filter.hpp:426-483)
+// ---------------------------------------------------------------------------
+namespace ipfc {
+namespace {
+
+// out += b, float (laplacian's sum of the two second derivatives)
+__global__ void __launch_bounds__(kThreads) add_f32_kernel(float* o, long long op, const float* b, long long bp,
+                                                           int rowlen) {
+    const int y = blockIdx.y;
+    float* ro = row_ptr_mut<float>(o, op, y);
+    const float* rb = reinterpret_cast<const float*>(reinterpret_cast<const char*>(b) + (long long)y * bp);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rowlen; q += gridDim.x * blockDim.x) ro[q] = ro[q] + rb[q];
+}
+
+// out = hypot(out, b) in float, rounded as the C library's hypotf rounds it:
+// sqrt(x^2 + y^2) evaluated in double (both squares exact) and rounded once
+// to float; an infinite operand gives +inf, a NaN propagates.
+__global__ void __launch_bounds__(kThreads) hypot_f32_kernel(float* o, long long op, const float* b, long long bp,
+                                                             int rowlen) {
+    const int y = blockIdx.y;
+    float* ro = row_ptr_mut<float>(o, op, y);
+    const float* rb = reinterpret_cast<const float*>(reinterpret_cast<const char*>(b) + (long long)y * bp);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rowlen; q += gridDim.x * blockDim.x) {
+        const float gx = ro[q], gy = rb[q];
+        float r;
+        if (isinf(gx) || isinf(gy)) {
+            r = INFINITY;
+        } else if (isnan(gx) || isnan(gy)) {
+            r = gx + gy;
+        } else {
+            const double dx = gx, dy = gy;
+            r = __double2float_rn(__dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy))));
+        }
+        ro[q] = r;
+    }
+}
+
+// out = saturate_cast<T>(|v - b| > threshold ? v + amount (v - b) : v), double
+template <typename T>
+__global__ void __launch_bounds__(kThreads) unsharp_kernel(const void* s, long long sp, const double* b, long long bp,
+                                                           void* o, long long op, int rowlen, double amount,
+                                                           double threshold) {
+    const int y = blockIdx.y;
+    const T* rs = row_ptr<T>(s, sp, y);
+    const double* rb = reinterpret_cast<const double*>(reinterpret_cast<const char*>(b) + (long long)y * bp);
+    T* ro = row_ptr_mut<T>(o, op, y);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < rowlen; q += gridDim.x * blockDim.x) {
+        const double v = (double)rs[q], diff = __dsub_rn(v, rb[q]);
+        ro[q] = sat_from_d<T>(fabs(diff) > threshold ? __dadd_rn(v, __dmul_rn(amount, diff)) : v);
+    }
+}
+
+dim3 rows_grid(int rowlen, int H) {
+    const int bx = (rowlen + kThreads - 1) / kThreads;
+    return dim3(bx < 16 ? bx : 16, H);
+}
+
+// A float destination of the source's shape (laplacian, gradientMagnitude).
+int check_f32_dst(const ipfc_image* src, const ipfc_image* dst, const char* fn) {
+    if (!src || !dst) return set_error(IPFC_ERR_INVALID, "ipf: %s: null image", fn);
+    if (dst->dtype != IPFC_F32)
+        return set_error(IPFC_ERR_INVALID, "ipf: %s: the result is float (ImageF)", fn);
+    return check_pair(src, dst, fn, false);
+}
+
+// Two derivative images of the staged source: into the result view and into
+// a float buffer, then a per-sample kernel joins them into the result.
+template <typename Join>
+int two_sobels(const ipfc_image* src, ipfc_image* dst, int dx0, int dy0, int dx1, int dy1, int ksize, double scale,
+               int border, void* stream, const char* fn, Join join) {
+    int rc = check_f32_dst(src, dst, fn);
+    if (rc == -1) return IPFC_OK;
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevView in, out;
+    if ((rc = view_in(src, s, &in, fn))) return rc;
+    if ((rc = view_out(dst, s, &out, fn))) {
+        finish(dst, &in, &out, s, fn);
+        return rc;
+    }
+    const int W = src->width, H = src->height, C = src->channels;
+    cudaError_t e = cudaSuccess;
+    {
+        DevBuf b;
+        e = b.alloc((long long)W * C * 4, H, s);
+        if (e == cudaSuccess) {
+            const ipfc_image vin = dev_image(in.ptr, W, H, C, src->dtype, in.pitch);
+            ipfc_image vo = dev_image(out.ptr, W, H, C, IPFC_F32, out.pitch);
+            ipfc_image vb = dev_image(b.p, W, H, C, IPFC_F32, b.pitch);
+            rc = ipfc_sobel(&vin, &vo, dx0, dy0, ksize, scale, border, s);
+            if (!rc) rc = ipfc_sobel(&vin, &vb, dx1, dy1, ksize, scale, border, s);
+            if (!rc) {
+                join(static_cast<float*>(out.ptr), out.pitch, static_cast<const float*>(b.p), b.pitch, W * C, H, s);
+                e = cudaGetLastError();
+            }
+        }
+    }
+    const int frc = finish(dst, &in, &out, s, fn);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_status(e, fn);
+    return frc;
+}
+
+}  // namespace
+}  // namespace ipfc
+
+extern "C" int ipfc_laplacian(const ipfc_image* src, ipfc_image* dst, int ksize, double scale, int border,
+                              void* stream) {
+    const char* fn = "laplacian";
+    if (ksize == 1) {
+        // filter2D<float> with {0,1,0, 1,-4,1, 0,1,0}, each tap (float)(tap * scale)
+        if (!src || !dst) return set_error(IPFC_ERR_INVALID, "ipf: %s: null image", fn);
+        if (dst->dtype != IPFC_F32) return set_error(IPFC_ERR_INVALID, "ipf: %s: the result is float (ImageF)", fn);
+        const float base[9] = {0, 1, 0, 1, -4, 1, 0, 1, 0};
+        float k[9];
+        for (int i = 0; i < 9; ++i) k[i] = (float)((double)base[i] * scale);
+        return ipfc_filter2d(src, dst, k, 3, 3, -1, -1, border, 0.0, 0.0, stream);
+    }
+    return two_sobels(src, dst, 2, 0, 0, 2, ksize, scale, border, stream, fn,
+                      [](float* o, long long op, const float* b, long long bp, int rowlen, int H, cudaStream_t s) {
+                          add_f32_kernel<<<rows_grid(rowlen, H), kThreads, 0, s>>>(o, op, b, bp, rowlen);
+                      });
+}
+
+extern "C" int ipfc_gradient_magnitude(const ipfc_image* src, ipfc_image* dst, int ksize, void* stream) {
+    return two_sobels(src, dst, 1, 0, 0, 1, ksize, 1.0, IPFC_BORDER_REFLECT101, stream, "gradientMagnitude",
+                      [](float* o, long long op, const float* b, long long bp, int rowlen, int H, cudaStream_t s) {
+                          hypot_f32_kernel<<<rows_grid(rowlen, H), kThreads, 0, s>>>(o, op, b, bp, rowlen);
+                      });
+}
+
+extern "C" int ipfc_unsharp_mask(const ipfc_image* src, ipfc_image* dst, double sigma, double amount, double threshold,
+                                 void* stream) {
+    const char* fn = "unsharpMask";
+    int rc = check_pair(src, dst, fn, true);
+    if (rc == -1) return IPFC_OK;
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevView in, out;
+    if ((rc = view_in(src, s, &in, fn))) return rc;
+    if ((rc = view_out(dst, s, &out, fn))) {
+        finish(dst, &in, &out, s, fn);
+        return rc;
+    }
+    const int W = src->width, H = src->height, C = src->channels;
+    cudaError_t e = cudaSuccess;
+    {
+        DevBuf blurred;
+        e = blurred.alloc((long long)W * C * 8, H, s);
+        if (e == cudaSuccess) {
+            // gaussianBlur<double>(src, sigma): FP64 in the reference's order
+            const ipfc_image vin = dev_image(in.ptr, W, H, C, src->dtype, in.pitch);
+            ipfc_image vb = dev_image(blurred.p, W, H, C, IPFC_F64, blurred.pitch);
+            rc = ipfc_gaussian_blur(&vin, &vb, sigma, 0.0, 0, IPFC_BORDER_REFLECT101, s);
+            if (!rc) {
+                e = by_type(src->dtype, [&](auto t) {
+                    unsharp_kernel<decltype(t)><<<rows_grid(W * C, H), kThreads, 0, s>>>(
+                        in.ptr, in.pitch, static_cast<const double*>(blurred.p), blurred.pitch, out.ptr, out.pitch,
+                        W * C, amount, threshold);
+                    return cudaGetLastError();
+                });
+            }
+        }
     }
     const int frc = finish(dst, &in, &out, s, fn);
     if (rc) return rc;

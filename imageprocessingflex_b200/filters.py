@@ -409,6 +409,35 @@ def pyrDown(src, stream=None):
     return dst
 
 
+def _float_result(fn, src, stream, *args):
+    lib = _lib.load()
+    sv, keep = _source(src)
+    dst, dv = _alloc(src, tuple(src.shape), F32)  # ImageF
+    _check(getattr(lib, fn)(ctypes.byref(sv), ctypes.byref(dv), *args, _stream_of(src, stream)))
+    del keep
+    return dst
+
+
+def laplacian(src, ksize=1, scale=1.0, border=BorderMode.Reflect101, stream=None):
+    """laplacian (filter.hpp:426-438): float32 result."""
+    return _float_result("ipfc_laplacian", src, stream, int(ksize), float(scale), int(border))
+
+
+def gradientMagnitude(src, ksize=3, stream=None):
+    """gradientMagnitude (filter.hpp:462-467): float32 result."""
+    return _float_result("ipfc_gradient_magnitude", src, stream, int(ksize))
+
+
+def unsharpMask(src, sigma=1.0, amount=1.0, threshold=0.0, stream=None):
+    """unsharpMask (filter.hpp:473-483): the source's type."""
+    lib = _lib.load()
+    sv, keep, dst, dv = _pair(src, None)
+    _check(lib.ipfc_unsharp_mask(ctypes.byref(sv), ctypes.byref(dv), float(sigma), float(amount), float(threshold),
+                                 _stream_of(src, stream)))
+    del keep
+    return dst
+
+
 def pyrUp(src, stream=None):
     """pyrUp (geometry.hpp:516-525): 2W x 2H."""
     lib = _lib.load()

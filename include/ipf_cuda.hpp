@@ -225,6 +225,33 @@ Image<T> pyrUp(const Image<T>& src) {
     return out;
 }
 
+/// laplacian (include/ipf/filter.hpp:426-438).
+template <class T>
+ImageF laplacian(const Image<T>& src, int ksize = 1, double scale = 1.0, BorderMode border = BorderMode::Reflect101) {
+    ImageF out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_laplacian(&s, &d, ksize, scale, static_cast<int>(border), nullptr));
+    return out;
+}
+
+/// gradientMagnitude (include/ipf/filter.hpp:462-467).
+template <class T>
+ImageF gradientMagnitude(const Image<T>& src, int ksize = 3) {
+    ImageF out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_gradient_magnitude(&s, &d, ksize, nullptr));
+    return out;
+}
+
+/// unsharpMask (include/ipf/filter.hpp:473-483).
+template <class T>
+Image<T> unsharpMask(const Image<T>& src, double sigma = 1.0, double amount = 1.0, double threshold = 0.0) {
+    Image<T> out(src.width(), src.height(), src.channels());
+    ipfc_image s = detail::view(src), d = detail::view(out);
+    detail::check(ipfc_unsharp_mask(&s, &d, sigma, amount, threshold, nullptr));
+    return out;
+}
+
 /// ssim (include/ipf/metrics.hpp:51-78).
 template <class T>
 double ssim(const Image<T>& a, const Image<T>& b, ImageF* ssimMap = nullptr) {

@@ -275,6 +275,21 @@ IPFC_API int ipfc_corner_min_eigen_val(const ipfc_image* src, ipfc_image* dst, i
 IPFC_API int ipfc_canny(const ipfc_image* src, ipfc_image* dst, double low_threshold, double high_threshold, int ksize,
                         int l2_gradient, void* stream);
 
+/* laplacian (filter.hpp:426-438): dst IPFC_F32.  ksize 1 is filter2D with
+ * the 3x3 kernel {0,1,0, 1,-4,1, 0,1,0} times scale; a larger ksize sums the
+ * second-order Sobel derivatives sobel(2,0) + sobel(0,2). */
+IPFC_API int ipfc_laplacian(const ipfc_image* src, ipfc_image* dst, int ksize, double scale, int border, void* stream);
+
+/* gradientMagnitude (filter.hpp:462-467): dst IPFC_F32, hypot of sobel(1,0)
+ * and sobel(0,1) (Reflect101), rounded as the C library's hypotf. */
+IPFC_API int ipfc_gradient_magnitude(const ipfc_image* src, ipfc_image* dst, int ksize, void* stream);
+
+/* unsharpMask (filter.hpp:473-483): dst of the source's type;
+ * out = saturate_cast(|v - b| > threshold ? v + amount (v - b) : v) with
+ * b = gaussianBlur<double>(src, sigma), all in FP64 as the reference. */
+IPFC_API int ipfc_unsharp_mask(const ipfc_image* src, ipfc_image* dst, double sigma, double amount, double threshold,
+                               void* stream);
+
 /* ---- batches: many images, a few launches --------------------------------
  *
  * No counterpart in the reference (ipf runs one call per image).  A batch

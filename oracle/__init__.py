@@ -265,6 +265,31 @@ class CpuFilters:
             raise ValueError(f"ipf: canny failed ({rc})")
         return out
 
+    def laplacian(self, src, ksize=1, scale=1.0, border=REFLECT101):
+        src = np.ascontiguousarray(src)
+        W, H, C = _shape(src)
+        out = np.zeros(src.shape, np.float32)
+        if self._f("laplacian")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out), ksize, _c_double(scale), border):
+            raise ValueError("ipf: laplacian failed")
+        return out
+
+    def gradient_magnitude(self, src, ksize=3):
+        src = np.ascontiguousarray(src)
+        W, H, C = _shape(src)
+        out = np.zeros(src.shape, np.float32)
+        if self._f("gradient_magnitude")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out), ksize):
+            raise ValueError("ipf: gradientMagnitude failed")
+        return out
+
+    def unsharp_mask(self, src, sigma=1.0, amount=1.0, threshold=0.0):
+        src = np.ascontiguousarray(src)
+        W, H, C = _shape(src)
+        out = np.zeros_like(src)
+        if self._f("unsharp_mask")(_ptr(src), DTYPE_CODE[src.dtype], W, H, C, _ptr(out), _c_double(sigma),
+                                   _c_double(amount), _c_double(threshold)):
+            raise ValueError("ipf: unsharpMask failed")
+        return out
+
     def box_filter(self, src, kw, kh, normalize=True, border=REFLECT101, border_value=0.0, out_dtype=None):
         src = np.ascontiguousarray(src)
         out = self._out(src, out_dtype)

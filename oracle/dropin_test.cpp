@@ -146,6 +146,11 @@ int main() {
     compare("pyrUp gray", cuda::pyrUp(gray), pyrUp(gray), 0, 0);
     compare("canny RGB 50 150", cuda::canny(rgb, 50.0, 150.0), canny(rgb, 50.0, 150.0), 0, 0);
     compare("cornerHarris gray", cuda::cornerHarris(gray), cornerHarris(gray), 0, 1e-5);
+    compare("laplacian ksize 1 RGB", cuda::laplacian(rgb), laplacian(rgb), 0, 1e-5);
+    compare("laplacian ksize 3 gray", cuda::laplacian(gray, 3), laplacian(gray, 3), 0, 0);
+    compare("gradientMagnitude RGB", cuda::gradientMagnitude(rgb), gradientMagnitude(rgb), 0, 0);
+    compare("unsharpMask RGB sigma 1.5 amount 0.8 threshold 3", cuda::unsharpMask(rgb, 1.5, 0.8, 3.0),
+            unsharpMask(rgb, 1.5, 0.8, 3.0), 0, 0);
     {
         ImageF mg, mr;
         const ImageU8 other = seeded<std::uint8_t>(1920, 1080, 3, 2);

@@ -893,3 +893,68 @@ int orc_canny(const void* src, int dt, int W, int H, int C, uint8_t* dst, double
     free(f); free(q);
     return ORC_OK;
 }
+
+/* filter.hpp:426-438 (laplacian): ksize 1 is filter2D<float> with the 3x3
+ * kernel {0,1,0, 1,-4,1, 0,1,0}, each tap (float)(tap * scale), default
+ * anchor, no delta; a larger ksize sums sobel(2, 0) and sobel(0, 2) in float. */
+int orc_laplacian(const void* src, int dt, int W, int H, int C, float* dst, int ksize, double scale, int border) {
+    if (W <= 0 || H <= 0) return ORC_OK;
+    if (ksize == 1) {
+        const float base[9] = {0, 1, 0, 1, -4, 1, 0, 1, 0};
+        float k[9];
+        for (int i = 0; i < 9; ++i) k[i] = (float)((double)base[i] * scale);
+        return orc_filter2d(src, dt, W, H, C, dst, ORC_F32, k, 3, 3, -1, -1, border, 0.0, 0.0);
+    }
+    const size_t n = (size_t)W * H * C;
+    float* b = (float*)malloc(n * sizeof(float));
+    if (!b) return ORC_ENOMEM;
+    int rc = sobel_f32(src, dt, W, H, C, dst, 2, 0, ksize, scale, border);
+    if (!rc) rc = sobel_f32(src, dt, W, H, C, b, 0, 2, ksize, scale, border);
+    if (!rc)
+        for (size_t i = 0; i < n; ++i) dst[i] += b[i];
+    free(b);
+    return rc;
+}
+
+/* filter.hpp:462-467 (gradientMagnitude) over magnitude (filter.hpp:440-446):
+ * hypot of sobel(1, 0) and sobel(0, 1) (Reflect101), in float. */
+int orc_gradient_magnitude(const void* src, int dt, int W, int H, int C, float* dst, int ksize) {
+    if (W <= 0 || H <= 0) return ORC_OK;
+    const size_t n = (size_t)W * H * C;
+    float* gy = (float*)malloc(n * sizeof(float));
+    if (!gy) return ORC_ENOMEM;
+    int rc = sobel_f32(src, dt, W, H, C, dst, 1, 0, ksize, 1.0, ORC_REFLECT101);
+    if (!rc) rc = sobel_f32(src, dt, W, H, C, gy, 0, 1, ksize, 1.0, ORC_REFLECT101);
+    if (!rc)
+        for (size_t i = 0; i < n; ++i) dst[i] = hypotf(dst[i], gy[i]);
+    free(gy);
+    return rc;
+}
+
+/* filter.hpp:473-483 (unsharpMask): blurred = gaussianBlur<double>(src,
+ * sigma) (Reflect101); out = saturate_cast<T>(|v - b| > threshold
+ * ? v + amount * (v - b) : v), every operation in double. */
+int orc_unsharp_mask(const void* src, int dt, int W, int H, int C, void* dst, double sigma, double amount,
+                     double threshold) {
+    if (W <= 0 || H <= 0) return ORC_OK;
+    const int nk = orc_gaussian_kernel_1d(sigma, 0, NULL, 0);  /* the length only */
+    if (nk < 0) return ORC_EINVAL;
+    double* k = (double*)malloc((size_t)nk * sizeof(double));
+    const size_t n = (size_t)W * H * C;
+    double* b = (double*)malloc(n * sizeof(double));
+    if (!k || !b) {
+        free(k);
+        free(b);
+        return ORC_ENOMEM;
+    }
+    orc_gaussian_kernel_1d(sigma, 0, k, nk);
+    int rc = orc_sep_filter(src, dt, W, H, C, b, ORC_F64, k, nk, k, nk, nk / 2, nk / 2, ORC_REFLECT101, 0.0, 0.0);
+    free(k);
+    if (!rc)
+        for (size_t i = 0; i < n; ++i) {
+            const double v = load_elem(src, dt, i), diff = v - b[i];
+            store_sat(dst, dt, i, fabs(diff) > threshold ? v + amount * diff : v);
+        }
+    free(b);
+    return rc;
+}

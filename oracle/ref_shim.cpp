@@ -294,4 +294,35 @@ int ref_canny(const void* src, int dt, int W, int H, int C, std::uint8_t* dst, d
     });
 }
 
+int ref_laplacian(const void* src, int dt, int W, int H, int C, float* dst, int ksize, double scale, int border) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::laplacian(wrap<S>(src, W, H, C), ksize, scale, static_cast<BorderMode>(border)), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_gradient_magnitude(const void* src, int dt, int W, int H, int C, float* dst, int ksize) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::gradientMagnitude(wrap<S>(src, W, H, C), ksize), dst);
+        });
+        return 0;
+    });
+}
+
+int ref_unsharp_mask(const void* src, int dt, int W, int H, int C, void* dst, double sigma, double amount,
+                     double threshold) {
+    return guard([&] {
+        dispatch(dt, [&](auto s) {
+            using S = decltype(s);
+            unwrap(ipf::unsharpMask(wrap<S>(src, W, H, C), sigma, amount, threshold), dst);
+        });
+        return 0;
+    });
+}
+
 }  // extern "C"

@@ -121,3 +121,34 @@ def test_callers_on_device_tensors(gpu, orc):
     np.testing.assert_array_equal(ipf.pyrDown(dev).cpu().numpy(), orc.pyr_down(img))
     np.testing.assert_array_equal(ipf.canny(dev, 20.0, 60.0).cpu().numpy(), orc.canny(img, 20.0, 60.0))
     np.testing.assert_array_equal(ipf.integralImage(dev).cpu().numpy(), orc.integral(img))
+
+
+@pytest.mark.parametrize("dt", DTYPES, ids=_ids)
+def test_laplacian_gradient_magnitude_unsharp_mask(gpu, orc, dt):
+    """laplacian, gradientMagnitude and unsharpMask against the oracle (pinned
+    to the compiled reference in test_oracle.py).  Exact where the GPU's sums
+    are exact or FP64 (integer sources with integer taps; int32 and double
+    sources; unsharpMask always, whose blur is FP64); otherwise FP32 against
+    the reference's FP64 sums, within 1e-5 of the result's scale."""
+    integer = dt in (np.uint8, np.uint16, np.int16, np.int32)
+    fp64 = dt in (np.int32, np.float64)
+
+    def check(got, want, exact, what):
+        if exact:
+            np.testing.assert_array_equal(got, want, err_msg=what)
+        else:
+            scale = max(1.0, float(np.abs(want).max(initial=0.0)))
+            np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-5 * scale, err_msg=what)
+
+    for w, h, c in SHAPES:
+        img = oracle.random_image(w, h, c, dt, 5 * w + 3 * h + c)
+        for ks in (1, 3, 5):
+            for sc in (1.0, 0.37):
+                for b in oracle.BORDERS:
+                    check(ipf.laplacian(img, ks, sc, ipf.BorderMode(b)), orc.laplacian(img, ks, sc, b),
+                          fp64 or (integer and sc == 1.0), f"laplacian ksize {ks} scale {sc} border {b} {w}x{h}x{c}")
+            check(ipf.gradientMagnitude(img, ks), orc.gradient_magnitude(img, ks), fp64 or integer,
+                  f"gradientMagnitude ksize {ks} {w}x{h}x{c}")
+        for sigma, amount, thr in ((1.0, 1.0, 0.0), (2.3, 0.6, 4.0), (0.5, 2.5, 0.01)):
+            np.testing.assert_array_equal(ipf.unsharpMask(img, sigma, amount, thr), orc.unsharp_mask(img, sigma, amount, thr),
+                                          err_msg=f"unsharpMask {sigma} {amount} {thr} {w}x{h}x{c}")

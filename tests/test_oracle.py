@@ -250,6 +250,26 @@ def test_restatement_matches_reference_callers(orc, refimpl, dt):
                                                       refimpl.adaptive_threshold(img, 200.0, method, tt, bs, cc))
 
 
+@pytest.mark.parametrize("dt", [np.uint8, np.uint16, np.int16, np.int32, np.float32, np.float64],
+                         ids=lambda d: np.dtype(d).name)
+def test_restatement_matches_reference_derivative_callers(orc, refimpl, dt):
+    """laplacian (ksize 1 through filter2D<float>, larger through sobel),
+    gradientMagnitude and unsharpMask: the restatement is bit-identical to the
+    reference."""
+    for (w, h, c) in ((1, 1, 1), (23, 17, 3), (40, 29, 1), (13, 31, 4)):
+        img = oracle.random_image(w, h, c, dt, 3 * w + h + c)
+        for ks in (1, 3, 5):
+            for sc in (1.0, 0.37):
+                for b in oracle.BORDERS:
+                    np.testing.assert_array_equal(orc.laplacian(img, ks, sc, b), refimpl.laplacian(img, ks, sc, b),
+                                                  err_msg=f"laplacian ksize {ks} scale {sc} border {b}")
+        for ks in (1, 3, 5, 7):
+            np.testing.assert_array_equal(orc.gradient_magnitude(img, ks), refimpl.gradient_magnitude(img, ks))
+        for sigma, amount, thr in ((1.0, 1.0, 0.0), (2.3, 0.6, 4.0), (0.5, 2.5, 0.01)):
+            np.testing.assert_array_equal(orc.unsharp_mask(img, sigma, amount, thr),
+                                          refimpl.unsharp_mask(img, sigma, amount, thr))
+
+
 def test_tap_generators_match_reference(orc, refimpl):
     for s in (0.3, 0.5, 1.0, 1.7, 2.0, 2.3, 4.0, 7.5):
         np.testing.assert_array_equal(orc.gaussian_kernel_1d(s), refimpl.gaussian_kernel_1d(s))
