@@ -21,6 +21,7 @@ from .filters import (  # noqa: F401
     cornerMinEigenVal,
     derivKernel,
     dilate,
+    emboss,
     erode,
     filter2D,
     gaussianBlur,
@@ -31,9 +32,12 @@ from .filters import (  # noqa: F401
     laplacian,
     medianBlur,
     morphologyEx,
+    prewitt,
     pyrDown,
     pyrUp,
+    scharr,
     sepFilter2D,
+    sharpen,
     sobel,
     ssim,
     unsharpMask,

@@ -418,6 +418,36 @@ def _float_result(fn, src, stream, *args):
     return dst
 
 
+def scharr(src, dx, dy, scale=1.0, border=BorderMode.Reflect101, stream=None):
+    """scharr (filter.hpp:411-414): float32, {-scale, 0, scale} x {3, 10, 3}."""
+    if not ((dx, dy) in ((1, 0), (0, 1))):
+        raise Error("ipf: scharr: (dx, dy) must be (1,0) or (0,1)")
+    d, s = [-scale, 0.0, scale], [3.0, 10.0, 3.0]
+    kx, ky = (d, s) if dx else (s, d)
+    return sepFilter2D(src, kx, ky, border, dtype=np.float32, stream=stream)
+
+
+def prewitt(src, dx, dy, border=BorderMode.Reflect101, stream=None):
+    """prewitt (filter.hpp:419-422): float32, {-1, 0, 1} x {1, 1, 1}."""
+    if not ((dx, dy) in ((1, 0), (0, 1))):
+        raise Error("ipf: prewitt: (dx, dy) must be (1,0) or (0,1)")
+    d, s = [-1.0, 0.0, 1.0], [1.0, 1.0, 1.0]
+    kx, ky = (d, s) if dx else (s, d)
+    return sepFilter2D(src, kx, ky, border, dtype=np.float32, stream=stream)
+
+
+def sharpen(src, strength=1.0, stream=None):
+    """sharpen (filter.hpp:487-490): filter2D with {0,-s,0, -s,1+4s,-s, 0,-s,0}, s = float(strength)."""
+    s = np.float32(strength)
+    k = np.array([[0, -s, 0], [-s, np.float32(1) + np.float32(4) * s, -s], [0, -s, 0]], np.float32)
+    return filter2D(src, k, stream=stream)
+
+
+def emboss(src, stream=None):
+    """emboss (filter.hpp:494-496): filter2D with {-2,-1,0, -1,1,1, 0,1,2}."""
+    return filter2D(src, np.array([[-2, -1, 0], [-1, 1, 1], [0, 1, 2]], np.float32), stream=stream)
+
+
 def laplacian(src, ksize=1, scale=1.0, border=BorderMode.Reflect101, stream=None):
     """laplacian (filter.hpp:426-438): float32 result."""
     return _float_result("ipfc_laplacian", src, stream, int(ksize), float(scale), int(border))

@@ -225,6 +225,36 @@ Image<T> pyrUp(const Image<T>& src) {
     return out;
 }
 
+/// scharr (include/ipf/filter.hpp:411-414): sepFilter2D<float> with
+/// {-scale, 0, scale} along the derivative axis and {3, 10, 3} across it.
+template <class T>
+ImageF scharr(const Image<T>& src, int dx, int dy, double scale = 1.0, BorderMode border = BorderMode::Reflect101) {
+    if (!((dx == 1 && dy == 0) || (dx == 0 && dy == 1))) throw Error("ipf: scharr: (dx, dy) must be (1,0) or (0,1)");
+    const std::vector<double> d = {-scale, 0.0, scale}, s = {3.0, 10.0, 3.0};
+    return dx ? ipf::cuda::sepFilter2D<float>(src, d, s, border) : ipf::cuda::sepFilter2D<float>(src, s, d, border);
+}
+
+/// prewitt (include/ipf/filter.hpp:419-422).
+template <class T>
+ImageF prewitt(const Image<T>& src, int dx, int dy, BorderMode border = BorderMode::Reflect101) {
+    if (!((dx == 1 && dy == 0) || (dx == 0 && dy == 1))) throw Error("ipf: prewitt: (dx, dy) must be (1,0) or (0,1)");
+    const std::vector<double> d = {-1.0, 0.0, 1.0}, s = {1.0, 1.0, 1.0};
+    return dx ? ipf::cuda::sepFilter2D<float>(src, d, s, border) : ipf::cuda::sepFilter2D<float>(src, s, d, border);
+}
+
+/// sharpen (include/ipf/filter.hpp:487-490): filter2D with the 3x3 Laplacian sharpening kernel.
+template <class T>
+Image<T> sharpen(const Image<T>& src, double strength = 1.0) {
+    const float s = static_cast<float>(strength);
+    return ipf::cuda::filter2D(src, makeKernel(3, 3, {0, -s, 0, -s, 1 + 4 * s, -s, 0, -s, 0}));
+}
+
+/// emboss (include/ipf/filter.hpp:494-496).
+template <class T>
+Image<T> emboss(const Image<T>& src) {
+    return ipf::cuda::filter2D(src, makeKernel(3, 3, {-2, -1, 0, -1, 1, 1, 0, 1, 2}));
+}
+
 /// laplacian (include/ipf/filter.hpp:426-438).
 template <class T>
 ImageF laplacian(const Image<T>& src, int ksize = 1, double scale = 1.0, BorderMode border = BorderMode::Reflect101) {

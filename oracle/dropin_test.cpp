@@ -146,6 +146,10 @@ int main() {
     compare("pyrUp gray", cuda::pyrUp(gray), pyrUp(gray), 0, 0);
     compare("canny RGB 50 150", cuda::canny(rgb, 50.0, 150.0), canny(rgb, 50.0, 150.0), 0, 0);
     compare("cornerHarris gray", cuda::cornerHarris(gray), cornerHarris(gray), 0, 1e-5);
+    compare("scharr dx RGB", cuda::scharr(rgb, 1, 0), scharr(rgb, 1, 0), 0, 0);
+    compare("prewitt dy gray", cuda::prewitt(gray, 0, 1), prewitt(gray, 0, 1), 0, 0);
+    compare("sharpen 0.7 RGB", cuda::sharpen(rgb, 0.7), sharpen(rgb, 0.7), 1, 0);
+    compare("emboss gray", cuda::emboss(gray), emboss(gray), 0, 0);
     compare("laplacian ksize 1 RGB", cuda::laplacian(rgb), laplacian(rgb), 0, 1e-5);
     compare("laplacian ksize 3 gray", cuda::laplacian(gray, 3), laplacian(gray, 3), 0, 0);
     compare("gradientMagnitude RGB", cuda::gradientMagnitude(rgb), gradientMagnitude(rgb), 0, 0);

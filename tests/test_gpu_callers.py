@@ -152,3 +152,25 @@ def test_laplacian_gradient_magnitude_unsharp_mask(gpu, orc, dt):
         for sigma, amount, thr in ((1.0, 1.0, 0.0), (2.3, 0.6, 4.0), (0.5, 2.5, 0.01)):
             np.testing.assert_array_equal(ipf.unsharpMask(img, sigma, amount, thr), orc.unsharp_mask(img, sigma, amount, thr),
                                           err_msg=f"unsharpMask {sigma} {amount} {thr} {w}x{h}x{c}")
+
+
+def test_scharr_prewitt_sharpen_emboss(gpu, orc):
+    """The thin wrappers over sepFilter2D<float> / filter2D against the
+    oracle with the reference's taps (filter.hpp:411-422, 487-496): exact with
+    integer taps on uint8, within 1 LSB for sharpen's fractional ones."""
+    for w, h, c in SHAPES:
+        img = oracle.random_image(w, h, c, np.uint8, 17 * w + h + c)
+        d, s = [-1.0, 0.0, 1.0], [3.0, 10.0, 3.0]
+        np.testing.assert_array_equal(ipf.scharr(img, 1, 0), orc.sep_filter(img, d, s, out_dtype=np.float32))
+        np.testing.assert_array_equal(ipf.scharr(img, 0, 1), orc.sep_filter(img, s, d, out_dtype=np.float32))
+        p = [1.0, 1.0, 1.0]
+        np.testing.assert_array_equal(ipf.prewitt(img, 1, 0), orc.sep_filter(img, d, p, out_dtype=np.float32))
+        np.testing.assert_array_equal(ipf.prewitt(img, 0, 1), orc.sep_filter(img, p, d, out_dtype=np.float32))
+        em = np.array([[-2, -1, 0], [-1, 1, 1], [0, 1, 2]], np.float32)
+        np.testing.assert_array_equal(ipf.emboss(img), orc.filter2d(img, em))
+        st = np.float32(0.7)
+        sk = np.array([[0, -st, 0], [-st, np.float32(1) + np.float32(4) * st, -st], [0, -st, 0]], np.float32)
+        diff = np.abs(ipf.sharpen(img, 0.7).astype(np.int32) - orc.filter2d(img, sk).astype(np.int32))
+        assert diff.max(initial=0) <= 1
+    with pytest.raises(ipf.Error, match="scharr"):
+        ipf.scharr(oracle.random_image(4, 4, 1, np.uint8, 1), 1, 1)
