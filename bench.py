@@ -375,7 +375,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                         else "fallback 6.65 TB/s", "kernel": "sep_tcol_kernel<13, 3> (tcgen05 column pass)",
+                         else "fallback 6.65 TB/s", "kernel": "sep_tcol_kernel<13, 3, false> (tcgen05 column pass, saturation compiled out)",
                          "alg_bytes_per_launch": int(alg_bytes), "ms_per_launch": round(ms_per_launch, 5)},
             "clocks": clk.summary(),
         }

@@ -162,7 +162,7 @@ __device__ __forceinline__ uint64_t tcol_fma2(uint64_t a, uint64_t b, uint64_t c
 //    pairs (2k-1, 2k) -- accumulators O[k], started at 0 -- and
 //    acc(o) = E + O at the end.
 // The FP32 sum order differs from one FMA chain only by that final add.
-template <int K, int C, int GH>
+template <int K, int C, int GH, bool CLAMP>
 __device__ __forceinline__ void tcol_row_chunk(const TcolArgs& a, const float (&v)[1 + 2 * GH][16],
                                                unsigned (&words)[4]) {
     constexpr int H2 = K / 2;
@@ -206,7 +206,7 @@ __device__ __forceinline__ void tcol_row_chunk(const TcolArgs& a, const float (&
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
             float x = acc[4 * t4 + t];
-            if (a.clamp) x = fminf(fmaxf(x, 0.f), 255.f);
+            if constexpr (CLAMP) x = fminf(fmaxf(x, 0.f), 255.f);
             const float r = __fadd_rd(x, 8388608.0f);
             wd = __byte_perm(wd, __float_as_uint(r), byte_insert_sel(t));
         }
@@ -216,7 +216,7 @@ __device__ __forceinline__ void tcol_row_chunk(const TcolArgs& a, const float (&
 
 }  // namespace
 
-template <int K, int C>
+template <int K, int C, bool CLAMP>
 __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_constant__ TcolArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     constexpr int KR = tcol_kr(K);
@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
                     });
                     static_for<0, NG>([&](auto I) { tcol_ld_wait(v[decltype(I)::value]); });
                     unsigned words[4];
-                    tcol_row_chunk<K, C, GH>(a, v, words);
+                    tcol_row_chunk<K, C, GH, CLAMP>(a, v, words);
                     const int xo = xs + 16 * j;
                     if (row_ok && xo < a.rowlen) {
                         if (a.vec_store && xo + 16 <= a.rowlen) {
@@ -489,22 +489,39 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
 
 namespace {
 
+// The split of the last (units, slabs per band, grid) this thread launched:
+// a run of calls on one image size bisects once.
 void tcol_split(TcolArgs& a, int grid) {
+    thread_local int c_units = -1, c_ns = -1, c_grid = -1;
+    thread_local int c_split[kTcolMaxCtas + 1];
+    if (a.units != c_units || a.ns != c_ns || grid != c_grid) {
+        tcol_split_units(a.units, a.ns, grid, c_split);
+        c_units = a.units;
+        c_ns = a.ns;
+        c_grid = grid;
+    }
     a.nsplit = grid;
-    tcol_split_units(a.units, a.ns, grid, a.split);
+    std::memcpy(a.split, c_split, sizeof(int) * (size_t)(grid + 1));
 }
 
+// The saturation is compiled out when the host has shown that every output
+// stays inside [0, 255] (non-negative taps whose product of sums keeps the
+// extreme inputs in range): the row pass then spends no issue slots on it.
 template <int K, int C>
 cudaError_t tcol_launch_kc(TcolArgs a, cudaStream_t s) {
-    static unsigned done = 0;
-    cudaError_t e = ensure_smem_attr((const void*)sep_tcol_kernel<K, C>, tcol_smem(K), &done);
+    static unsigned done[2] = {0, 0};
+    const void* fn = a.clamp ? (const void*)sep_tcol_kernel<K, C, true> : (const void*)sep_tcol_kernel<K, C, false>;
+    cudaError_t e = ensure_smem_attr(fn, tcol_smem(K), &done[a.clamp ? 1 : 0]);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     const int grid = a.units < sms ? a.units : sms;
     if (grid <= kTcolMaxCtas) tcol_split(a, grid);
-    sep_tcol_kernel<K, C><<<grid, kTcolThreads, tcol_smem(K), s>>>(a);
+    if (a.clamp)
+        sep_tcol_kernel<K, C, true><<<grid, kTcolThreads, tcol_smem(K), s>>>(a);
+    else
+        sep_tcol_kernel<K, C, false><<<grid, kTcolThreads, tcol_smem(K), s>>>(a);
     return cudaGetLastError();
 }
 

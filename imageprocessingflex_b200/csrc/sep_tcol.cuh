@@ -135,32 +135,57 @@ struct TcolWalk {
     }
 };
 
-// Splits the (band, slab) units into `grid` contiguous ranges of about
-// equal cost: split[b] .. split[b+1]-1 is range b (split has grid + 1
-// entries).  A unit costs one step; the last slab of a band also pays for
-// the right halo at the image's edge, whose border-resolved gathers take
-// about as long as kTcolEdgeCost slab steps (measured), and every range pays
-// its own left and right halo steps.  Every range gets at least one unit
-// (grid <= units).
-constexpr double kTcolEdgeCost = 2.5;
+// Splits the (band, slab) units into `grid` contiguous ranges whose
+// largest estimated cost is as small as it can be: split[b] .. split[b+1]-1
+// is range b (split has grid + 1 entries); every range gets at least one
+// unit (grid <= units).  The kernel's time is its slowest CTA's, so the
+// split minimises the bottleneck rather than matching an average share.
+// Costs are in slab steps, from per-CTA timings of 4K RGB launches: a unit
+// costs one step; a range starting at a band's first slab pays the left
+// image-edge halo step (border-resolved gathers), kTcolLeftEdgeCost more; a
+// band's last slab pays the right one, kTcolRightEdgeCost more; a range that
+// runs on into the next band pays that band's left edge with
+// kTcolBandCrossCost off (the two edge steps overlap in the pipeline); and
+// every range pays its own left and right halo steps.
+constexpr double kTcolLeftEdgeCost = 1.9;
+constexpr double kTcolRightEdgeCost = 1.3;
+constexpr double kTcolBandCrossCost = -0.6;
 constexpr double kTcolHaloCost = 0.3;
-inline void tcol_split_units(int units, int ns, int grid, int* split) {
-    auto cost = [&](int u) { return 1.0 + (u % ns == ns - 1 ? kTcolEdgeCost : 0.0); };
-    double total = 0;
-    for (int u = 0; u < units; ++u) total += cost(u);
-    total += 2 * kTcolHaloCost * grid;
-    const double share = total / grid;
-    split[0] = 0;
-    int u = 0;
-    double done = 0;  // cost of the units before u, with the halos of the ranges so far
-    for (int b = 1; b < grid; ++b) {
-        done += 2 * kTcolHaloCost;
-        // range b-1 ends where the running cost is nearest b shares; at
-        // least one unit per range, and one left for each range after it
-        while (u < units - (grid - b) && (split[b - 1] == u || done + 0.5 * cost(u) <= b * share)) done += cost(u++);
-        split[b] = u;
-    }
-    split[grid] = units;
+// Cost of units [0, u) counted as later units of a range (no range start).
+inline double tcol_cost_prefix(int u, int ns) {
+    return (double)u + kTcolRightEdgeCost * (double)(u / ns) +
+           (kTcolLeftEdgeCost + kTcolBandCrossCost) * (double)((u + ns - 1) / ns);
 }
-
+// Estimated cost of the range of units [u0, u1), u0 < u1.
+inline double tcol_range_cost(int u0, int u1, int ns) {
+    return 2 * kTcolHaloCost + tcol_cost_prefix(u1, ns) - tcol_cost_prefix(u0, ns) -
+           (u0 % ns == 0 ? kTcolBandCrossCost : 0.0);
+}
+// Greedy fill under a cost cap: each range takes the most units whose cost
+// stays within cap (at least one, and one left for every later range).
+// Returns whether the ranges hold every unit.
+inline bool tcol_fill_units(int units, int ns, int grid, double cap, int* split) {
+    split[0] = 0;
+    for (int b = 0; b < grid; ++b) {
+        const int u0 = split[b];
+        int lo = u0 + 1, hi = units - (grid - 1 - b);  // the range's possible ends
+        while (lo < hi) {  // the range cost grows with its end
+            const int mid = lo + (hi - lo + 1) / 2;
+            if (tcol_range_cost(u0, mid, ns) <= cap) lo = mid;
+            else hi = mid - 1;
+        }
+        split[b + 1] = lo;
+    }
+    return split[grid] == units;
+}
+inline void tcol_split_units(int units, int ns, int grid, int* split) {
+    // a cap above the whole image's cost always fits: bisect down from it
+    double lo = 0.0, hi = tcol_range_cost(0, units, ns) + 1.0 + kTcolLeftEdgeCost + kTcolRightEdgeCost;
+    while (hi - lo > 1e-3 * (1.0 + lo)) {
+        const double mid = 0.5 * (lo + hi);
+        if (tcol_fill_units(units, ns, grid, mid, split)) hi = mid;
+        else lo = mid;
+    }
+    tcol_fill_units(units, ns, grid, hi, split);
+}
 }  // namespace ipfc

@@ -21,6 +21,7 @@
 // never empty and within two edge units of the average cost.
 //
 // Prints "ok <cases>" and exits 0, or the first failures and exits 1.
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <algorithm>
@@ -142,9 +143,9 @@ static void check_k(int K, std::mt19937& rng) {
     }
 }
 
-// The host's cost-balanced unit split: contiguous, every range non-empty,
-// and no range costing more than the average share plus one edge unit and
-// its halos (the split's granularity).
+// The host's bottleneck unit split: contiguous, every range non-empty,
+// range costs as tcol_range_cost sums them, and no range costing more than
+// the mean plus one costliest unit (the split's granularity).
 static void check_split(std::mt19937& rng) {
     for (int t = 0; t < 3000; ++t) {
         const int nb = 1 + (int)(rng() % 40), ns = 1 + (int)(rng() % 120);
@@ -152,18 +153,25 @@ static void check_split(std::mt19937& rng) {
         const int grid = 1 + (int)(rng() % std::min(units, 160));
         std::vector<int> split(grid + 1, -1);
         tcol_split_units(units, ns, grid, split.data());
-        double total = 2 * kTcolHaloCost * grid, worst = 0;
-        auto cost = [&](int u) { return 1.0 + (u % ns == ns - 1 ? kTcolEdgeCost : 0.0); };
-        for (int u = 0; u < units; ++u) total += cost(u);
         if (split[0] != 0 || split[grid] != units) fail("split ends", split[0], split[grid], units);
+        double total = 0, worst = 0;
         for (int b = 0; b < grid; ++b) {
             if (split[b + 1] <= split[b]) fail("empty or reversed range", b, split[b], split[b + 1]);
+            // the range cost against a unit-by-unit sum
             double c = 2 * kTcolHaloCost;
-            for (int u = split[b]; u < split[b + 1]; ++u) c += cost(u);
+            for (int u = split[b]; u < split[b + 1]; ++u) {
+                c += 1.0;
+                if (u % ns == ns - 1) c += kTcolRightEdgeCost;
+                if (u % ns == 0) c += kTcolLeftEdgeCost + (u == split[b] ? 0.0 : kTcolBandCrossCost);
+            }
+            if (std::fabs(c - tcol_range_cost(split[b], split[b + 1], ns)) > 1e-9) fail("range cost", b, split[b], split[b + 1]);
+            total += c;
             worst = std::max(worst, c);
         }
         ++cases;
-        if (worst > total / grid + 2 * (1.0 + kTcolEdgeCost) + 1e-9) fail("unbalanced split", units, grid, (int)worst);
+        // the bottleneck stays within one costliest unit of the mean
+        if (worst > total / grid + 1.0 + kTcolLeftEdgeCost + kTcolRightEdgeCost + 1e-9)
+            fail("unbalanced split", units, grid, (int)worst);
     }
 }
 
