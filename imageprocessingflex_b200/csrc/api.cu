@@ -311,16 +311,31 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
                      const double* kx, const double* ky, int K, int border, double delta, double bv, int clamp,
                      cudaStream_t s, cudaError_t* err);
 
-// Kernel selection for separable filters.  Default: uint8 -> uint8 calls on
-// images of at least kTcolMinSamples samples that the tensor-core
-// column-pass kernel covers (sep_tcol.cu) run there where it is the faster
-// one (from 9 taps on 3 or 4 channels, from 15 on one channel; gaussianBlur
-// sigma 2 on 3840x2160x3: 1.34x), the rest on the CUDA-core fast kernel
-// where it is instantiated, else on the generic kernels.
+// Kernel selection for separable filters.  Default: uint8 -> uint8 calls
+// that the tensor-core column-pass kernel covers (sep_tcol.cu) run there
+// where it is the faster one (tcol_wins), the rest on the CUDA-core fast
+// kernel where it is instantiated, else on the generic kernels.
 // IPFC_SEP_PATH=generic forces the generic fused/two-pass kernels; =fast
 // keeps uint8 calls off the tensor cores; =tcol takes the tensor-core kernel
 // for every size it covers.
-constexpr long long kTcolMinSamples = 1LL << 22;
+//
+// The tensor-core kernel costs about 11 us per CTA on top of its per-unit
+// work and barely depends on the tap count; the CUDA-core kernel scales
+// with samples x taps.  Measured gaussianBlur, uint8, L2-cold inputs (us per
+// image, CUDA-core / tensor-core):
+//   C = 1: 1920x1080 K 13  16.6 / 22.8   3840x2160 K 9  30.0 / 28.2
+//          3840x2160 K 13  29.7 / 28.9   4096x4096 K 9  48.4 / 38.9
+//   C = 3: 1920x1080 K 13  21.8 / 27.5   2560x1440 K 9  31.1 / 33.5
+//          2560x1440 K 13  35.2 / 35.0   2560x1440 K 15 40.9 / 35.5
+//          3840x2160 K 9   59.2 / 48.4   3840x2160 K 13 64.7 / 50.3
+//   C = 4: 1920x1080 K 15  27.5 / 28.4   2560x1440 K 13 38.9 / 38.5
+//          3840x2160 K 9   68.9 / 59.1
+// Below 9 taps the CUDA-core kernel stays (3840x2160x3 K 7: 49.4 / 51.6).
+static bool tcol_wins(int kw, int channels, long long samples) {
+    if (kw < 9) return false;
+    if (channels == 1) return samples >= 7000000;
+    return samples >= 16000000 || (kw >= 13 && samples >= 10000000);
+}
 // Callers that share the GPU among many streams (the request server) keep
 // separable calls on the CUDA-core kernel: the tensor-core kernel is
 // persistent, one CTA with 203 KB of shared memory on every SM, so while it
@@ -427,13 +442,8 @@ static bool run_sep_fast(const ipfc_image* src, const ipfc_image* dst, const Dev
                             &f))
         return false;
     const int mode = sep_path_mode();
-    // measured on 3840x2160 (µs per image, CUDA-core / tensor-core): C = 3 --
-    // K 7: 49.4 / 51.6, K 9: 57.9 / 52.3, K 13: 63.8 / 54.9; C = 1 -- K 13:
-    // 28.9 / 31.8, K 15: 33.8 / 32.5.  The tensor-core kernel's cost barely
-    // depends on K, the CUDA-core kernel's grows with it.
-    const bool tcol_wins = kw >= (src->channels == 1 ? 15 : 9);
-    const bool tcol = mode == 4 || (mode == 0 && !t_shared_gpu && tcol_wins &&
-                                    (long long)src->width * src->channels * src->height >= kTcolMinSamples);
+    const bool tcol = mode == 4 || (mode == 0 && !t_shared_gpu &&
+                                    tcol_wins(kw, src->channels, (long long)src->width * src->channels * src->height));
     if (tcol && src->dtype == IPFC_U8 && dst->dtype == IPFC_U8 &&
         sep_tcol_launch(in.ptr, in.pitch, out.ptr, out.pitch, src->width, src->height, src->channels, kx, ky, kw,
                         border, delta, bv, f.clamp, s, e))
