@@ -322,8 +322,10 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
         // ------------------------------------------------------------ producers
         // Each lane loads and converts the same items of every step -- rows
         // 8 kg + r8 for its warp's kg, samples n .. n+15 -- into registers
-        // one step ahead: the loads of step g+1 are in flight while step g
-        // waits for its B buffer and converts.
+        // one step ahead: the loads of step g+1 are issued as soon as step g
+        // is handed over, and land while the warp waits for step g+1's B
+        // buffer.  One register buffer: copying a second one into it at the
+        // end of each step would make the hand-over wait for the loads.
         const int pw = warp - 1, r8 = lane & 7, c4 = lane >> 3;
         static_assert(kTcolProdWarps % 2 == 0, "the items of one warp share the half of the slab");
         const int n = 64 * (pw & 1) + 16 * c4;  // this lane's chunk of the slab
@@ -365,8 +367,6 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
         int g = 0;
         while (walk.next(st)) {
             if (*abort_flag) break;
-            uint4 nxt[PER];
-            if (ahead.next(sa)) load(sa, nxt);
             const int bb = g & 1;
             if (g >= 2 && !tcol_wait(&bempty[bb], (unsigned)((g - 2) >> 1) & 1u, a, abort_flag)) break;
             unsigned char* B = sm + tcol_off_b(bb, K);
@@ -389,8 +389,9 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
             }
             fence_async_smem();
             mbar_arrive(&bfull[bb]);
-#pragma unroll
-            for (int r = 0; r < PER; ++r) cur[r] = nxt[r];
+            // the next step's items, in flight while this warp waits for
+            // that step's B buffer
+            if (ahead.next(sa)) load(sa, cur);
             ++g;
         }
     } else {
