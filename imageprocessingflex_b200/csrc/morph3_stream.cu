@@ -137,7 +137,12 @@ __global__ void __launch_bounds__(32 * kM3Warps) morph3_stream_kernel(const Morp
     hrow(load(y0 - 1), pe, po);
     hrow(load(y0), ce, co);
     Raw r1 = load(y0 + 1), r2 = load(y0 + 2);
-    for (int y = y0; y < y1; ++y) {
+    // Unrolled over the band, so the row registers rotate by renaming: a
+    // copy of r2 into r1 would wait for r2's loads to land.
+#pragma unroll
+    for (int i = 0; i < kM3Band; ++i) {
+        const int y = y0 + i;
+        if (y >= y1) break;
         unsigned ne[4], no[4];
         hrow(r1, ne, no);
         r1 = r2;
