@@ -330,7 +330,8 @@ bool sep_tcol_launch(const void* src, long long spitch, void* dst, long long dpi
 //          3840x2160 K 9   59.2 / 48.4   3840x2160 K 13 64.7 / 50.3
 //   C = 4: 1920x1080 K 15  27.5 / 28.4   2560x1440 K 13 38.9 / 38.5
 //          3840x2160 K 9   68.9 / 59.1
-// Below 9 taps the CUDA-core kernel stays (3840x2160x3 K 7: 49.4 / 51.6).
+// Below 9 taps the CUDA-core kernel stays (3840x2160x3 K 7 on an earlier
+// build of the tensor-core kernel: 49.4 / 51.6).
 static bool tcol_wins(int kw, int channels, long long samples) {
     if (kw < 9) return false;
     if (channels == 1) return samples >= 7000000;

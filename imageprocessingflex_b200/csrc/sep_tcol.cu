@@ -324,8 +324,9 @@ __global__ void __launch_bounds__(kTcolThreads, 1) sep_tcol_kernel(const __grid_
         // 8 kg + r8 for its warp's kg, samples n .. n+15 -- into registers
         // one step ahead: the loads of step g+1 are issued as soon as step g
         // is handed over, and land while the warp waits for step g+1's B
-        // buffer.  One register buffer: copying a second one into it at the
-        // end of each step would make the hand-over wait for the loads.
+        // buffer.  One register buffer: with a second one copied into it at
+        // the end of each step, the copy stalled on those loads and the
+        // hand-overs came 1-2 us later (measured per warp).
         const int pw = warp - 1, r8 = lane & 7, c4 = lane >> 3;
         static_assert(kTcolProdWarps % 2 == 0, "the items of one warp share the half of the slab");
         const int n = 64 * (pw & 1) + 16 * c4;  // this lane's chunk of the slab
